@@ -1,0 +1,137 @@
+/* tmsolve: B200-native twisted-mass Wilson operator and solvers behind a
+ * plain C ABI.
+ *
+ * Each entry point replaces one entry point of the reference library nissa
+ * (paths relative to its src/ directory).  Buffers are the reference's own
+ * CPU (AoS) layout in float64:
+ *   lx conf    V x [mu][row][col][re,im]            (LxField<quad_su3>)
+ *   eo conf    [par][Vh] x [mu][row][col][re,im]    (EoField<quad_su3>)
+ *   lx spinor  V x [spin][col][re,im]               (LxField<spincolor>)
+ *   eo spinor  Vh x [spin][col][re,im]              (EvnField/OddField<spincolor>)
+ * with sites numbered as the reference numbers them (lx: t slowest, z
+ * fastest; e/o: lx order within each parity).  By default the pointers are
+ * host pointers (copied in and out on every call); after
+ * tms_set_pointer_mode(ctx, TMS_PTR_DEVICE) they are device pointers to the
+ * same layout.  Every function returns a tms_status; none throws.
+ *
+ * Residues are SQUARED relative residues, |r|^2/|b|^2, as in the reference
+ * (inverters/templates/cg_invert_template_threaded.hpp:129).
+ */
+#ifndef TMSOLVE_H
+#define TMSOLVE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum
+{
+  TMS_OK = 0,
+  TMS_ERR_NOT_CONVERGED = 1, /* reference: CRASH("exit without converging") */
+  TMS_ERR_NAN = 2,           /* reference: CRASH("nanned") */
+  TMS_ERR_BAD_ARG = 3,
+  TMS_ERR_OOM = 4,
+  TMS_ERR_TIMEOUT = 5,
+  TMS_ERR_CUDA = 6,
+  TMS_ERR_NO_CONF = 7,
+  TMS_ERR_INVALID_SOURCE = 8 /* reference: CRASH("invalid norm") */
+} tms_status;
+
+typedef enum
+{
+  TMS_PREC_DOUBLE = 0,      /* plain FP64 CG, the reference's arithmetic */
+  TMS_PREC_MIXED_SINGLE = 1,/* FP32 inner CG, 12-real links, FP64 reliable updates */
+  TMS_PREC_MIXED_HALF = 2   /* FP16 spinors with per-site FP32 scale, FP64 reliable updates */
+} tms_precision;
+
+typedef enum { TMS_LAYOUT_LX = 0, TMS_LAYOUT_EO = 1 } tms_layout;
+typedef enum { TMS_PTR_HOST = 0, TMS_PTR_DEVICE = 1 } tms_ptr_mode;
+
+/* conf upload flags */
+#define TMS_CONF_BC_INCLUDED 1 /* links already carry the time boundary sign, as the reference's operators see them */
+
+typedef struct
+{
+  int32_t status;           /* tms_status of the solve */
+  int32_t iterations;       /* inner CG iterations (the reference's final_iter) */
+  int32_t reliable_updates; /* FP64 residual recomputations (mixed precision) */
+  int32_t pad;
+  double iterated_rel_res2; /* |r_iterated|^2/|b|^2 at exit */
+  double true_rel_res2;     /* |b - A x|^2/|b|^2 recomputed in FP64 at exit */
+  double lx_rel_res2;       /* full solves: |g5 Q x - src|^2/|src|^2 in lx (cg_invert_tmD_eoprec.cpp:192-212) */
+  double seconds;           /* device time of the solve */
+} tms_stats;
+
+typedef struct tms_ctx tms_ctx;
+
+/* ---- context: one lattice, one resident gauge configuration, one stream ---- */
+
+/* Lattice T x L^3 on CUDA device `device`; time boundary sign bc_t (-1 antiperiodic, +1 periodic).
+ * Replaces initGrid(T,L) (base/init.cpp:563-798) and the e/o geometry it builds
+ * (geometry/geometry_eo.cpp:41-100), per instance instead of process-global. */
+tms_status tms_create(tms_ctx **ctx, int T, int L, double bc_t, int device);
+/* General T x LX x LY x LZ form (all even). */
+tms_status tms_create4(tms_ctx **ctx, int T, int LX, int LY, int LZ, double bc_t, int device);
+tms_status tms_destroy(tms_ctx *ctx);
+const char *tms_last_error(const tms_ctx *ctx);
+tms_status tms_set_pointer_mode(tms_ctx *ctx, int mode);
+int64_t tms_volume(const tms_ctx *ctx);
+
+/* Device copies of the reference's geometry tables, for bit-exact checks against
+ * loclx_parity/loceo_of_loclx/loclx_of_loceo/loceo_neighup/loceo_neighdw
+ * (geometry/geometry_eo.cpp:66-100).  Host int32 outputs: parity[V], eo_of_lx[V],
+ * lx_of_eo[2*Vh], neighup[2*Vh*4], neighdw[2*Vh*4]; any may be NULL. */
+tms_status tms_geometry_tables(tms_ctx *ctx, int32_t *parity, int32_t *eo_of_lx, int32_t *lx_of_eo,
+                               int32_t *neighup, int32_t *neighdw);
+
+/* Upload the gauge configuration (kept resident until replaced or destroyed).
+ * Replaces the conf argument of every operator and split_lx_vector_into_eo_parts
+ * of the conf (geometry/geometry_mix.hpp:46-60, done once here instead of per call). */
+tms_status tms_conf_upload(tms_ctx *ctx, const double *conf, int layout, int flags);
+/* 1 if the links are special unitary (12-real reconstruction enabled for FP32), 0 if not */
+int tms_conf_is_su3(const tms_ctx *ctx);
+
+/* ---- operators (e/o) ---- */
+
+/* tmn2Deo_or_tmn2Doe_eos: dirac_operators/tmD_eoprec/dirac_operator_tmD_eoprec_portable.hpp:33-169.
+ * out (parity par_out) = -2 x hopping of in (opposite parity). has_anis=0: no anisotropy. */
+tms_status tms_hop_eo(tms_ctx *ctx, int par_out, const double *in, double *out, int has_anis, double anis);
+/* tmDee_or_oo_eos / inv_tmDee_or_oo_eos: ..._portable.hpp:171-222 */
+tms_status tms_tmDee(tms_ctx *ctx, double kappa, double mu, const double *in, double *out);
+tms_status tms_inv_tmDee(tms_ctx *ctx, double kappa, double mu, const double *in, double *out);
+/* tmDkern_eoprec_eos: dirac_operator_tmD_eoprec_portable.cpp:36-51 (odd -> odd) */
+tms_status tms_kern_eoprec(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu, const double *in,
+                           double *out);
+/* tmDkern_eoprec_square_eos: dirac_operator_tmD_eoprec_portable.cpp:54-65, K(+mu)K(-mu) */
+tms_status tms_kern_eoprec_square(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu,
+                                  const double *in, double *out);
+
+/* ---- operators (full lattice, lx spinors) ---- */
+
+/* apply_tmQ: dirac_operators/tmQ/dirac_operator_tmQ_portable.cpp:29-176 */
+tms_status tms_apply_tmQ(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu, const double *in,
+                         double *out);
+/* apply_tmQ2: Q(+mu)Q(-mu), dirac_operators/tmQ2/dirac_operator_tmQ2.cpp:17-30 (a stub in the
+ * reference; the body there, and apply_tmclovQ2 at zero clover, tmclovQ2/dirac_operator_tmclovQ2.hpp:13-24) */
+tms_status tms_apply_tmQ2(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu, const double *in,
+                          double *out);
+
+/* ---- solvers ---- */
+
+/* inv_tmDkern_eoprec_square_eos_cg: inverters/twisted_mass/cg_invert_tmD_eoprec.cpp:61-78
+ * Solves K(+mu)K(-mu) sol = src on odd sites.  guess may be NULL (sol starts at 0);
+ * stops when |r|^2 < residue |src|^2 or after niter iterations. */
+tms_status tms_cg_eoprec_square(tms_ctx *ctx, double *sol, const double *guess, const double *src, double kappa,
+                                int has_anis, double anis, double mu, int niter, double residue, int precision,
+                                tms_stats *stats);
+/* inv_tmD_cg_eoprec: inverters/twisted_mass/cg_invert_tmD_eoprec.cpp:102-213
+ * Full solve D_tm sol = src on lx spinors via Eq. (8)-(11) of the e/o preconditioning. */
+tms_status tms_cg_eoprec(tms_ctx *ctx, double *sol_lx, const double *src_lx, double kappa, int has_anis,
+                         double anis, double mu, int niter, double residue, int precision, tms_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,66 @@
+"""ctypes binding of libtmsolve.so (the C ABI declared in include/tmsolve.h)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import build as _build
+
+_lib = None
+
+P = ctypes.c_void_p
+D = ctypes.c_double
+I = ctypes.c_int
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("iterations", ctypes.c_int32), ("reliable_updates", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("iterated_rel_res2", ctypes.c_double), ("true_rel_res2", ctypes.c_double),
+                ("lx_rel_res2", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "tms_create": (I, [ctypes.POINTER(P), I, I, D, I]),
+    "tms_create4": (I, [ctypes.POINTER(P), I, I, I, I, D, I]),
+    "tms_destroy": (I, [P]),
+    "tms_last_error": (ctypes.c_char_p, [P]),
+    "tms_set_pointer_mode": (I, [P, I]),
+    "tms_volume": (ctypes.c_int64, [P]),
+    "tms_geometry_tables": (I, [P, P, P, P, P, P]),
+    "tms_conf_upload": (I, [P, P, I, I]),
+    "tms_conf_is_su3": (I, [P]),
+    "tms_hop_eo": (I, [P, I, P, P, I, D]),
+    "tms_tmDee": (I, [P, D, D, P, P]),
+    "tms_inv_tmDee": (I, [P, D, D, P, P]),
+    "tms_kern_eoprec": (I, [P, D, I, D, D, P, P]),
+    "tms_kern_eoprec_square": (I, [P, D, I, D, D, P, P]),
+    "tms_apply_tmQ": (I, [P, D, I, D, D, P, P]),
+    "tms_apply_tmQ2": (I, [P, D, I, D, D, P, P]),
+    "tms_cg_eoprec_square": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
+    "tms_cg_eoprec": (I, [P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
+}
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load libtmsolve.so (building it first if it is missing or stale)."""
+    global _lib
+    if _lib is None:
+        if build_if_missing and _build.stale():
+            _build.build()
+        if not os.path.exists(_build.LIB):
+            raise RuntimeError("libtmsolve.so is not built (python -m nissa_b200.build)")
+        L = ctypes.CDLL(_build.LIB)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

@@ -1,0 +1,668 @@
+// Hopping stencil with fused epilogues, fused CG linear algebra and
+// deterministic FP64 reductions.
+//
+// One thread computes one output site.  The stencil body gathers the eight
+// neighbours directly from the structure-of-arrays planes: along z and y the
+// neighbours of a warp are contiguous, along x and t they are a whole row /
+// time slice away, which for the volumes served here sits in the 126 MB L2,
+// so each input spinor and link crosses HBM about once per launch.  The
+// antiperiodic time boundary is a sign applied in the kernel when a hop
+// crosses t = T-1 -> 0 (links are stored periodic).
+//
+// Every kernel whose result feeds a global scalar (alpha, beta, |r|^2) reduces
+// per block in FP64 with warp shuffles, and the last block to finish sums the
+// block partials in a fixed order: the result does not depend on scheduling
+// and no block ever waits for another.
+#pragma once
+
+#include "tms_common.cuh"
+
+namespace tms
+{
+  constexpr int HOP_THREADS = 128;
+
+  // -------------------------------------------------- FP64 block reduction
+  __device__ __forceinline__ double warp_sum(double v)
+  {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  }
+
+  // Reduce v over the grid.  The last block to finish calls fin(total) from
+  // thread 0.  Must be reached by every thread of every block.
+  template <int NT, class Fin>
+  __device__ __forceinline__ void grid_reduce(double v, const Reducer& red, const Fin& fin)
+  {
+    __shared__ double sh[NT / 32];
+    __shared__ bool amLast;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0)
+      {
+        double w = (lane < NT / 32) ? sh[lane] : 0.0;
+        w = warp_sum(w);
+        if (lane == 0)
+          {
+            red.partial[blockIdx.x] = w;
+            __threadfence();
+            const unsigned ticket = atomicAdd(red.counter, 1u);
+            amLast = (ticket == gridDim.x - 1);
+          }
+      }
+    __syncthreads();
+    if (amLast)
+      {
+        __threadfence();
+        double s = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) s += ((volatile double*)red.partial)[i];
+        s = warp_sum(s);
+        if (lane == 0) sh[warp] = s;
+        __syncthreads();
+        if (threadIdx.x == 0)
+          {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < NT / 32; w++) t += sh[w];
+            *red.result = t;
+            *red.counter = 0u;
+            fin(t);
+          }
+      }
+  }
+
+  struct NoFin
+  {
+    __device__ void operator()(double) const {}
+  };
+
+  // pick the accessor of parity p by value (keeps it in registers, no local-memory array)
+  template <class T>
+  __device__ __forceinline__ T pick(const T& a0, const T& a1, int p)
+  {
+    T r;
+    r.d = p ? a1.d : a0.d;
+    r.n = p ? a1.n : a0.n;
+    r.stride = a0.stride;
+    return r;
+  }
+
+  // ------------------------------------------------------- stencil body
+  // Accumulates the -2*hopping term sum_mu [(1-g_mu) U_x,mu in(x+mu) + (1+g_mu) U^+_x-mu,mu in(x-mu)]
+  // in the reference's chiral basis; projection and reconstruction tables follow
+  // dirac_operator_tmD_eoprec_portable.hpp:56-166.
+  template <int MU, bool FWD, typename R>
+  __device__ __forceinline__ void project(const C<R> s[12], C<R> h0[3], C<R> h1[3])
+  {
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      {
+        const C<R> s0 = s[c], s1 = s[3 + c], s2 = s[6 + c], s3 = s[9 + c];
+        if (FWD)
+          {
+            if (MU == 0) { h0[c] = cadd(s0, s2); h1[c] = cadd(s1, s3); }
+            if (MU == 1) { h0[c] = ciadd(s0, s3); h1[c] = ciadd(s1, s2); }
+            if (MU == 2) { h0[c] = cadd(s0, s3); h1[c] = csub(s1, s2); }
+            if (MU == 3) { h0[c] = ciadd(s0, s2); h1[c] = cisub(s1, s3); }
+          }
+        else
+          {
+            if (MU == 0) { h0[c] = csub(s0, s2); h1[c] = csub(s1, s3); }
+            if (MU == 1) { h0[c] = cisub(s0, s3); h1[c] = cisub(s1, s2); }
+            if (MU == 2) { h0[c] = csub(s0, s3); h1[c] = cadd(s1, s2); }
+            if (MU == 3) { h0[c] = cisub(s0, s2); h1[c] = ciadd(s1, s3); }
+          }
+      }
+  }
+
+  template <int MU, bool FWD, typename R>
+  __device__ __forceinline__ void reconstruct(C<R> acc[12], const C<R> u0[3], const C<R> u1[3])
+  {
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      {
+        acc[c] = cadd(acc[c], u0[c]);
+        acc[3 + c] = cadd(acc[3 + c], u1[c]);
+        if (FWD)
+          {
+            if (MU == 0) { acc[6 + c] = cadd(acc[6 + c], u0[c]); acc[9 + c] = cadd(acc[9 + c], u1[c]); }
+            if (MU == 1) { acc[6 + c] = cisub(acc[6 + c], u1[c]); acc[9 + c] = cisub(acc[9 + c], u0[c]); }
+            if (MU == 2) { acc[6 + c] = csub(acc[6 + c], u1[c]); acc[9 + c] = cadd(acc[9 + c], u0[c]); }
+            if (MU == 3) { acc[6 + c] = cisub(acc[6 + c], u0[c]); acc[9 + c] = ciadd(acc[9 + c], u1[c]); }
+          }
+        else
+          {
+            if (MU == 0) { acc[6 + c] = csub(acc[6 + c], u0[c]); acc[9 + c] = csub(acc[9 + c], u1[c]); }
+            if (MU == 1) { acc[6 + c] = ciadd(acc[6 + c], u1[c]); acc[9 + c] = ciadd(acc[9 + c], u0[c]); }
+            if (MU == 2) { acc[6 + c] = cadd(acc[6 + c], u1[c]); acc[9 + c] = csub(acc[9 + c], u0[c]); }
+            if (MU == 3) { acc[6 + c] = ciadd(acc[6 + c], u0[c]); acc[9 + c] = cisub(acc[9 + c], u1[c]); }
+          }
+      }
+  }
+
+  // u = U h (FWD) or U^+ h (backward), times a real factor
+  template <bool FWD, typename R>
+  __device__ __forceinline__ void link_mul(const C<R> U[9], const C<R> h[3], C<R> u[3], R f)
+  {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+      {
+        C<R> a;
+        if (FWD)
+          {
+            a = cmul(U[3 * i], h[0]);
+            a = cadd(a, cmul(U[3 * i + 1], h[1]));
+            a = cadd(a, cmul(U[3 * i + 2], h[2]));
+          }
+        else
+          {
+            a = cjmul(U[i], h[0]);
+            a = cadd(a, cjmul(U[3 + i], h[1]));
+            a = cadd(a, cjmul(U[6 + i], h[2]));
+          }
+        u[i] = cscale(a, f);
+      }
+  }
+
+  template <int MU, int P, int LF>
+  __device__ __forceinline__ void hop_dir(const Lattice& g, const Site& s, int p, int ieo, const SpinorT<P>& in,
+                                          const LinkT<LF>& U, typename SpinorT<P>::R anis,
+                                          C<typename SpinorT<P>::R> acc[12])
+  {
+    using R = typename SpinorT<P>::R;
+    const R fmu = (MU > 0) ? anis : R(1);
+    {
+      bool w;
+      const int n = nbr_up<MU>(g, s, w);
+      C<R> sp[12], h0[3], h1[3], u0[3], u1[3], L[9];
+      in.load(n, sp);
+      project<MU, true>(sp, h0, h1);
+      U.load(p, MU, ieo, L);
+      const R f = w ? fmu * R(g.bc_t) : fmu;
+      link_mul<true>(L, h0, u0, f);
+      link_mul<true>(L, h1, u1, f);
+      reconstruct<MU, true>(acc, u0, u1);
+    }
+    {
+      bool w;
+      const int n = nbr_dw<MU>(g, s, w);
+      C<R> sp[12], h0[3], h1[3], u0[3], u1[3], L[9];
+      in.load(n, sp);
+      project<MU, false>(sp, h0, h1);
+      U.load(1 - p, MU, n, L);
+      const R f = w ? fmu * R(g.bc_t) : fmu;
+      link_mul<false>(L, h0, u0, f);
+      link_mul<false>(L, h1, u1, f);
+      reconstruct<MU, false>(acc, u0, u1);
+    }
+  }
+
+  template <int P, int LF>
+  __device__ __forceinline__ void hop_site(const Lattice& g, int p, int ieo, const SpinorT<P>& in, const LinkT<LF>& U,
+                                           typename SpinorT<P>::R anis, C<typename SpinorT<P>::R> acc[12])
+  {
+    using R = typename SpinorT<P>::R;
+#pragma unroll
+    for (int c = 0; c < 12; c++) acc[c] = {R(0), R(0)};
+    const Site s = eo_site(g, p, ieo);
+    hop_dir<0, P, LF>(g, s, p, ieo, in, U, anis, acc);
+    hop_dir<1, P, LF>(g, s, p, ieo, in, U, anis, acc);
+    hop_dir<2, P, LF>(g, s, p, ieo, in, U, anis, acc);
+    hop_dir<3, P, LF>(g, s, p, ieo, in, U, anis, acc);
+  }
+
+  // ------------------------------------------------------------ epilogues
+  // Each epilogue consumes the accumulated hop of one site (parity p, index
+  // ieo) and returns its contribution to the kernel's reduction (if any).
+
+  template <typename R>
+  __device__ __forceinline__ C<R> zdiag(const OpParams& o, double sgn)
+  {
+    return {R(1.0 / (2.0 * o.kappa)), R(sgn * o.mu)};
+  }
+  template <typename R>
+  __device__ __forceinline__ C<R> zinvdiag(const OpParams& o, double sgn)
+  {
+    const double a = 1.0 / (2.0 * o.kappa), b = sgn * o.mu, nrm = a * a + b * b;
+    return {R(+a / nrm), R(-b / nrm)};
+  }
+  // (z on spins 0,1; conj(z) on spins 2,3): tmDee_or_oo_eos, ..._portable.hpp:171-195
+  template <typename R>
+  __device__ __forceinline__ C<R> diag_apply(C<R> v, C<R> z, int c)
+  {
+    return (c < 6) ? cmul(v, z) : cmul(v, cconj(z));
+  }
+
+  // out = hop (tmn2Deo_or_tmn2Doe_eos)
+  template <int P>
+  struct EpiPlain
+  {
+    static constexpr bool kReduce = false;
+    SpinorT<P> out[2];
+    __device__ __forceinline__ double operator()(int p, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      pick(out[0], out[1], p).store(ieo, acc);
+      return 0.0;
+    }
+  };
+
+  // out = (1/2k + i s mu g5)^-1 hop  (inv_tmDee_or_oo_eos applied to the hop)
+  template <int P>
+  struct EpiInvDiag
+  {
+    static constexpr bool kReduce = false;
+    SpinorT<P> out[2];
+    const OpParams* prm;
+    double sgn;
+    __device__ __forceinline__ double operator()(int p, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const C<R> z = zinvdiag<R>(*prm, sgn);
+#pragma unroll
+      for (int c = 0; c < 12; c++) acc[c] = diag_apply(acc[c], z, c);
+      pick(out[0], out[1], p).store(ieo, acc);
+      return 0.0;
+    }
+  };
+
+  // out = g5 ( (1/2k + i s mu g5) x - hop/4 ), the Schur operator K_oo
+  // (tmDkern_eoprec_eos with ..._put_together_and_include_gamma5,
+  // dirac_operator_tmD_eoprec_portable.cpp:18-51).  Optionally reduces |out|^2.
+  template <int P, bool RED>
+  struct EpiKern
+  {
+    static constexpr bool kReduce = RED;
+    SpinorT<P> out[2];
+    SpinorT<P> x[2];
+    const OpParams* prm;
+    double sgn;
+    __device__ __forceinline__ double operator()(int p, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const C<R> z = zdiag<R>(*prm, sgn);
+      C<R> xv[12];
+      pick(x[0], x[1], p).load(ieo, xv);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> d = diag_apply(xv[c], z, c);
+          const C<R> q = cscale(acc[c], R(0.25));
+          acc[c] = (c < 6) ? csub(d, q) : csub(q, d);
+          if (RED) n2 += (double)acc[c].re * acc[c].re + (double)acc[c].im * acc[c].im;
+        }
+      pick(out[0], out[1], p).store(ieo, acc);
+      return n2;
+    }
+  };
+
+  // varphi = g5 (eta_o + hop/2): Eq. (8b), cg_invert_tmD_eoprec.cpp:37-58
+  template <int P>
+  struct EpiSrcPrep
+  {
+    static constexpr bool kReduce = false;
+    SpinorT<P> out[2];
+    SpinorT<P> eta[2];
+    __device__ __forceinline__ double operator()(int p, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      C<R> e[12];
+      pick(eta[0], eta[1], p).load(ieo, e);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> h = cscale(acc[c], R(0.5));
+          acc[c] = (c < 6) ? cadd(e[c], h) : csub(cscale(e[c], R(-1)), h);
+        }
+      pick(out[0], out[1], p).store(ieo, acc);
+      return 0.0;
+    }
+  };
+
+  // psi_e = (1/2k + i mu g5)^-1 (eta_e + hop/2): Eq. (11), cg_invert_tmD_eoprec.cpp:81-99 and :144-145
+  template <int P>
+  struct EpiReco
+  {
+    static constexpr bool kReduce = false;
+    SpinorT<P> out[2];
+    SpinorT<P> eta[2];
+    const OpParams* prm;
+    double sgn;
+    __device__ __forceinline__ double operator()(int p, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const C<R> z = zinvdiag<R>(*prm, sgn);
+      C<R> e[12];
+      pick(eta[0], eta[1], p).load(ieo, e);
+#pragma unroll
+      for (int c = 0; c < 12; c++) acc[c] = diag_apply(cadd(e[c], cscale(acc[c], R(0.5))), z, c);
+      pick(out[0], out[1], p).store(ieo, acc);
+      return 0.0;
+    }
+  };
+
+  // Full-lattice Q = g5 D_tm in the twisted basis (apply_tmQ,
+  // dirac_operator_tmQ_portable.cpp:160-174): spins 0,1: -hop/2 + kcf in + i m in;
+  // spins 2,3: +hop/2 - kcf in + i m in.  Optionally reduces |out|^2.
+  template <int P, bool RED>
+  struct EpiTmQ
+  {
+    static constexpr bool kReduce = RED;
+    SpinorT<P> out[2];
+    SpinorT<P> x[2];
+    const OpParams* prm;
+    double sgn;
+    __device__ __forceinline__ double operator()(int p, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const R kcf = R(1.0 / (2.0 * prm->kappa)), m = R(sgn * prm->mu);
+      C<R> xv[12];
+      pick(x[0], x[1], p).load(ieo, xv);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> im = {-m * xv[c].im, m * xv[c].re};
+          const C<R> h = cscale(acc[c], R(0.5));
+          const C<R> k = cscale(xv[c], kcf);
+          acc[c] = (c < 6) ? cadd(csub(k, h), im) : cadd(csub(h, k), im);
+          if (RED) n2 += (double)acc[c].re * acc[c].re + (double)acc[c].im * acc[c].im;
+        }
+      pick(out[0], out[1], p).store(ieo, acc);
+      return n2;
+    }
+  };
+
+  // ------------------------------------------------------ solver state
+  struct CgState
+  {
+    double rr;         // current iterated |r|^2
+    double rr_prev;    // |r|^2 of the previous iteration
+    double pAp;        // (p, A p)
+    double alpha;      // step length
+    double beta;       // direction update
+    double target;     // stop when rr < target (residue * |b|^2)
+    double rel_trigger;// reliable update when rr < rel_trigger
+    double b2;         // |b|^2
+    int iter;          // iterations done
+    int niter_max;
+    int stop;          // 0 running, 1 converged, 2 max iterations, 3 reliable update due, 4 breakdown
+    int pad;
+  };
+
+  enum StopCode { STOP_RUN = 0, STOP_CONVERGED = 1, STOP_MAXITER = 2, STOP_RELIABLE = 3, STOP_BREAKDOWN = 4 };
+
+  // alpha = rr / (p, A p)
+  struct FinAlpha
+  {
+    CgState* st;
+    __device__ void operator()(double pAp) const
+    {
+      st->pAp = pAp;
+      if (!(pAp > 0.0) || isnan(pAp))
+        {
+          st->stop = STOP_BREAKDOWN;
+          return;
+        }
+      st->alpha = st->rr / pAp;
+    }
+  };
+
+  // new |r|^2: beta, iteration count and the stopping tests of
+  // cg_invert_template_threaded.hpp:104-129
+  struct FinBeta
+  {
+    CgState* st;
+    __device__ void operator()(double rr) const
+    {
+      st->rr_prev = st->rr;
+      st->rr = rr;
+      st->beta = rr / st->rr_prev;
+      st->iter += 1;
+      if (isnan(rr) || isnan(st->beta)) st->stop = STOP_BREAKDOWN;
+      else if (rr < st->target) st->stop = STOP_CONVERGED;
+      else if (st->iter >= st->niter_max) st->stop = STOP_MAXITER;
+      else if (rr < st->rel_trigger) st->stop = STOP_RELIABLE;
+    }
+  };
+
+  // Second half of K(+mu)K(-mu) fused with the CG update:
+  //   s = K(+mu) t1 ;  x += alpha p ;  r -= alpha s ;  reduce |r|^2
+  // (cg_invert_template_threaded.hpp:82-107).  x may be kept in a wider
+  // precision (PX) than the iterated vectors (P).
+  template <int P, int PX>
+  struct EpiKernCgUpdate
+  {
+    static constexpr bool kReduce = true;
+    SpinorT<P> t1;    // the input of K(+mu) at the output site
+    SpinorT<P> r, p;
+    SpinorT<PX> x;
+    const OpParams* prm;
+    const CgState* st;
+    double sgn;
+    __device__ __forceinline__ double operator()(int par, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      using RX = typename SpinorT<PX>::R;
+      const C<R> z = zdiag<R>(*prm, sgn);
+      const R alpha = R(st->alpha);
+      C<R> v[12];
+      t1.load(ieo, v);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> d = diag_apply(v[c], z, c);
+          const C<R> q = cscale(acc[c], R(0.25));
+          acc[c] = (c < 6) ? csub(d, q) : csub(q, d); // s
+        }
+      r.load(ieo, v);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          v[c] = csub(v[c], cscale(acc[c], alpha));
+          n2 += (double)v[c].re * v[c].re + (double)v[c].im * v[c].im;
+        }
+      r.store(ieo, v);
+      p.load(ieo, v);
+      C<RX> xv[12];
+      x.load(ieo, xv);
+      const RX ax = RX(st->alpha);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          xv[c].re += ax * RX(v[c].re);
+          xv[c].im += ax * RX(v[c].im);
+        }
+      x.store(ieo, xv);
+      return n2;
+    }
+  };
+
+  // ---------------------------------------------------------- hop kernel
+  // Launch: one thread per output site; npar = 1 computes the parity
+  // par_out only, npar = 2 both parities (grid over 2*Vh).
+  template <int P, int LF, class Epi, class Fin>
+  __global__ void __launch_bounds__(HOP_THREADS)
+    hop_kernel(Lattice g, int par_out, int npar, SpinorT<P> in_e, SpinorT<P> in_o, LinkT<LF> U, const OpParams* prm,
+               Epi epi, Reducer red, Fin fin, const int* __restrict__ stop)
+  {
+    using R = typename SpinorT<P>::R;
+    if (stop && *stop) return;
+    const int idx = blockIdx.x * HOP_THREADS + threadIdx.x;
+    int p = par_out, ieo = idx;
+    if (npar == 2)
+      {
+        p = (idx >= g.Vh) ? 1 : 0;
+        ieo = idx - (p ? (int)g.Vh : 0);
+      }
+    const bool active = (idx < npar * g.Vh);
+    double part = 0.0;
+    if (active)
+      {
+        C<R> acc[12];
+        const R anis = R(prm->anis);
+        hop_site<P, LF>(g, p, ieo, p ? in_e : in_o, U, anis, acc);
+        part = epi(p, ieo, acc);
+      }
+    if (Epi::kReduce) grid_reduce<HOP_THREADS>(part, red, fin);
+  }
+
+  // ------------------------------------------------------- BLAS kernels
+  constexpr int BLAS_THREADS = 256;
+
+  // p = r + beta p  (cg_invert_template_threaded.hpp:115-124)
+  template <int P>
+  __global__ void __launch_bounds__(BLAS_THREADS)
+    xpay_kernel(int n, SpinorT<P> r, SpinorT<P> p, const CgState* st, const int* __restrict__ stop)
+  {
+    using R = typename SpinorT<P>::R;
+    if (stop && *stop) return;
+    const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
+    if (i >= n) return;
+    const R beta = R(st->beta);
+    C<R> a[12], b[12];
+    r.load(i, a);
+    p.load(i, b);
+#pragma unroll
+    for (int c = 0; c < 12; c++) b[c] = cadd(a[c], cscale(b[c], beta));
+    p.store(i, b);
+  }
+
+  // generic: reduce |a|^2 (or Re(a,b)) over n sites
+  template <int P, bool DOT>
+  __global__ void __launch_bounds__(BLAS_THREADS)
+    norm_kernel(int n, SpinorT<P> a, SpinorT<P> b, Reducer red)
+  {
+    using R = typename SpinorT<P>::R;
+    const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
+    double s = 0.0;
+    if (i < n)
+      {
+        C<R> x[12];
+        a.load(i, x);
+        if (DOT)
+          {
+            C<R> y[12];
+            b.load(i, y);
+#pragma unroll
+            for (int c = 0; c < 12; c++) s += (double)x[c].re * y[c].re + (double)x[c].im * y[c].im;
+          }
+        else
+#pragma unroll
+          for (int c = 0; c < 12; c++) s += (double)x[c].re * x[c].re + (double)x[c].im * x[c].im;
+      }
+    grid_reduce<BLAS_THREADS>(s, red, NoFin{});
+  }
+
+  // out = a*x + b*y (any precisions)
+  template <int PO, int PX, int PY>
+  __global__ void __launch_bounds__(BLAS_THREADS)
+    axpby_kernel(int n, double a, SpinorT<PX> x, double b, SpinorT<PY> y, SpinorT<PO> out)
+  {
+    using RO = typename SpinorT<PO>::R;
+    using RX = typename SpinorT<PX>::R;
+    using RY = typename SpinorT<PY>::R;
+    const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
+    if (i >= n) return;
+    C<RX> u[12];
+    C<RY> v[12];
+    C<RO> w[12];
+    x.load(i, u);
+    if (b != 0.0) y.load(i, v);
+#pragma unroll
+    for (int c = 0; c < 12; c++)
+      {
+        double re = a * (double)u[c].re, im = a * (double)u[c].im;
+        if (b != 0.0)
+          {
+            re += b * (double)v[c].re;
+            im += b * (double)v[c].im;
+          }
+        w[c] = {RO(re), RO(im)};
+      }
+    out.store(i, w);
+  }
+
+  // r = b - s and reduce |r|^2 (true residual), FP64
+  __global__ void __launch_bounds__(BLAS_THREADS)
+    residual_kernel(int n, SpinorT<PREC_F64> b, SpinorT<PREC_F64> s, SpinorT<PREC_F64> r, Reducer red)
+  {
+    const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
+    double acc = 0.0;
+    if (i < n)
+      {
+        C<double> u[12], v[12];
+        b.load(i, u);
+        s.load(i, v);
+#pragma unroll
+        for (int c = 0; c < 12; c++)
+          {
+            u[c] = csub(u[c], v[c]);
+            acc += u[c].re * u[c].re + u[c].im * u[c].im;
+          }
+        r.store(i, u);
+      }
+    grid_reduce<BLAS_THREADS>(acc, red, NoFin{});
+  }
+
+  // reduce |g5 q - eta|^2 (the lx residual check of cg_invert_tmD_eoprec.cpp:192-212)
+  __global__ void __launch_bounds__(BLAS_THREADS)
+    g5_residual_kernel(int n, SpinorT<PREC_F64> q, SpinorT<PREC_F64> eta, Reducer red)
+  {
+    const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
+    double acc = 0.0;
+    if (i < n)
+      {
+        C<double> u[12], v[12];
+        q.load(i, u);
+        eta.load(i, v);
+#pragma unroll
+        for (int c = 0; c < 12; c++)
+          {
+            const C<double> g = (c < 6) ? u[c] : cscale(u[c], -1.0);
+            const C<double> d = csub(g, v[c]);
+            acc += d.re * d.re + d.im * d.im;
+          }
+      }
+    grid_reduce<BLAS_THREADS>(acc, red, NoFin{});
+  }
+
+  // --------------------------------------------------- layout conversion
+  // host-order AoS doubles (site-major, 24 per site) <-> SoA device spinor.
+  // site_map (optional) gives the AoS row of SoA site i (used for lx <-> eo).
+  template <int P>
+  __global__ void aos_to_soa_kernel(int n, const double* __restrict__ aos, const int* __restrict__ site_map,
+                                    SpinorT<P> out)
+  {
+    using R = typename SpinorT<P>::R;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t row = site_map ? (size_t)site_map[i] : (size_t)i;
+    const double2* a = reinterpret_cast<const double2*>(aos + row * 24);
+    C<R> v[12];
+#pragma unroll
+    for (int c = 0; c < 12; c++)
+      {
+        const double2 w = a[c];
+        v[c] = {R(w.x), R(w.y)};
+      }
+    out.store(i, v);
+  }
+
+  template <int P>
+  __global__ void soa_to_aos_kernel(int n, SpinorT<P> in, const int* __restrict__ site_map, double* __restrict__ aos)
+  {
+    using R = typename SpinorT<P>::R;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t row = site_map ? (size_t)site_map[i] : (size_t)i;
+    C<R> v[12];
+    in.load(i, v);
+    double2* a = reinterpret_cast<double2*>(aos + row * 24);
+#pragma unroll
+    for (int c = 0; c < 12; c++) a[c] = make_double2((double)v[c].re, (double)v[c].im);
+  }
+}

@@ -1,0 +1,229 @@
+"""Host-side mirror of the reference's twisted-mass interface.
+
+Method names, argument meanings and error behaviour follow the reference
+library nissa (paths relative to its src/):
+
+  tmn2Deo_or_tmn2Doe_eos          dirac_operators/tmD_eoprec/dirac_operator_tmD_eoprec_portable.hpp:33-169
+  tmDee_or_oo_eos / inv_...       dirac_operator_tmD_eoprec_portable.hpp:171-222
+  tmDkern_eoprec_eos              dirac_operator_tmD_eoprec_portable.cpp:36-51
+  tmDkern_eoprec_square_eos       dirac_operator_tmD_eoprec_portable.cpp:54-65
+  apply_tmQ / apply_tmQ2          dirac_operators/tmQ/dirac_operator_tmQ_portable.cpp:29-176, tmQ2/dirac_operator_tmQ2.cpp
+  inv_tmDkern_eoprec_square_eos_cg inverters/twisted_mass/cg_invert_tmD_eoprec.cpp:61-78
+  inv_tmD_cg_eoprec               inverters/twisted_mass/cg_invert_tmD_eoprec.cpp:152-213
+
+The reference CRASHes on a non-converged solve, a NaN or an invalid source
+norm; here the same conditions raise TmError (with the status code of the C
+ABI).  ``residue`` is the squared relative residue, as in the reference.
+Every call goes through the C ABI of libtmsolve.so: there is no CPU path.
+
+Arrays are numpy float64 (host) or torch float64 tensors (host or CUDA) in the
+reference's CPU layout: eo spinor (Vh, 4, 3, 2), lx spinor (V, 4, 3, 2),
+lx conf (V, 4, 3, 3, 2), eo conf (2, Vh, 4, 3, 3, 2).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+STATUS = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN", 3: "BAD_ARG", 4: "OOM", 5: "TIMEOUT", 6: "CUDA_ERROR",
+          7: "NO_CONF", 8: "INVALID_SOURCE"}
+PRECISION = {"double": 0, "single": 1, "half": 2}
+
+
+class TmError(RuntimeError):
+    def __init__(self, status: int, message: str, stats: dict | None = None, result=None):
+        super().__init__("%s: %s" % (STATUS.get(status, status), message))
+        self.status = status
+        self.stats = stats
+        self.result = result
+
+
+def _is_torch(a):
+    return type(a).__module__.startswith("torch")
+
+
+class _Buf:
+    """Pointer + pointer-mode of an input/output array."""
+
+    def __init__(self, a, shape=None, out=False):
+        self.keep = None
+        if a is None:
+            self.ptr, self.device = None, False
+            return
+        if _is_torch(a):
+            if not a.is_contiguous() or str(a.dtype) != "torch.float64":
+                raise TypeError("torch tensors must be contiguous float64")
+            self.ptr, self.device = a.data_ptr(), a.is_cuda
+            self.keep = a
+        else:
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                if out:
+                    raise TypeError("output arrays must be contiguous float64 numpy arrays")
+                a = np.ascontiguousarray(a, dtype=np.float64)
+            self.ptr, self.device = a.ctypes.data, False
+            self.keep = a
+        if shape is not None and int(np.prod(shape)) != (a.numel() if _is_torch(a) else a.size):
+            raise ValueError("array has %d elements, expected shape %s" % (
+                a.numel() if _is_torch(a) else a.size, tuple(shape)))
+
+
+class Lattice:
+    """One T x LX x LY x LZ lattice with a resident gauge configuration on one GPU.
+
+    The per-instance counterpart of the reference's initGrid(T, L) plus its
+    e/o geometry (base/init.cpp:563-798, geometry/geometry_eo.cpp:41-100).
+    ``bc_t`` is the time boundary sign (-1 antiperiodic), applied in the
+    stencil when a hop crosses the time boundary."""
+
+    def __init__(self, T: int, L: int, bc_t: float = -1.0, device: int = 0, LX=None, LY=None, LZ=None):
+        self.lib = _lib.load()
+        self.T = T
+        self.LX, self.LY, self.LZ = LX or L, LY or L, LZ or L
+        self.V = T * self.LX * self.LY * self.LZ
+        self.Vh = self.V // 2
+        self.bc_t = bc_t
+        h = ctypes.c_void_p()
+        st = self.lib.tms_create4(ctypes.byref(h), T, self.LX, self.LY, self.LZ, float(bc_t), device)
+        if st != 0:
+            raise TmError(st, "tms_create(T=%d, L=%s)" % (T, (self.LX, self.LY, self.LZ)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tms_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------ helpers
+    def _check(self, st, what, stats=None, result=None):
+        if st != 0:
+            msg = self.lib.tms_last_error(self.h)
+            raise TmError(st, "%s: %s" % (what, msg.decode() if msg else ""), stats, result)
+
+    def _mode(self, *bufs):
+        dev = [b.device for b in bufs if b.ptr is not None]
+        if dev and any(d != dev[0] for d in dev):
+            raise TypeError("mixing host and device arrays in one call")
+        mode = 1 if (dev and dev[0]) else 0
+        self.lib.tms_set_pointer_mode(self.h, mode)
+        return mode
+
+    def _new_out(self, like, shape):
+        if like is not None and _is_torch(like):
+            import torch
+            return torch.empty(shape, dtype=torch.float64, device=like.device)
+        return np.empty(shape, np.float64)
+
+    @staticmethod
+    def _anis(anis):
+        return (0, 1.0) if anis is None else (1, float(anis))
+
+    # --------------------------------------------------------------- conf
+    def upload_conf(self, conf, layout: str = "lx", bc_included: bool = False):
+        """Make ``conf`` the resident gauge configuration.  With bc_included the
+        links already carry the time boundary sign (the form in which the
+        reference's operators see them); it is divided out and re-applied in the
+        stencil."""
+        shape = (self.V, 4, 3, 3, 2) if layout == "lx" else (2, self.Vh, 4, 3, 3, 2)
+        b = _Buf(conf, shape)
+        self._mode(b)
+        st = self.lib.tms_conf_upload(self.h, b.ptr, 0 if layout == "lx" else 1, 1 if bc_included else 0)
+        self._check(st, "tms_conf_upload")
+
+    @property
+    def conf_is_su3(self) -> bool:
+        return bool(self.lib.tms_conf_is_su3(self.h))
+
+    def geometry_tables(self):
+        V = self.V
+        t = dict(parity=np.empty(V, np.int32), eo_of_lx=np.empty(V, np.int32), lx_of_eo=np.empty((2, V // 2), np.int32),
+                 neighup_eo=np.empty((2, V // 2, 4), np.int32), neighdw_eo=np.empty((2, V // 2, 4), np.int32))
+        st = self.lib.tms_geometry_tables(self.h, *[t[k].ctypes.data for k in ("parity", "eo_of_lx", "lx_of_eo",
+                                                                                   "neighup_eo", "neighdw_eo")])
+        self._check(st, "tms_geometry_tables")
+        return t
+
+    # ---------------------------------------------------------- operators
+    def _unary(self, fn, args, inp, shape, out=None):
+        i = _Buf(inp, shape)
+        o = self._new_out(inp, shape) if out is None else out
+        ob = _Buf(o, shape, out=True)
+        self._mode(i, ob)
+        self._check(fn(self.h, *args(i.ptr, ob.ptr)), fn.__name__)
+        return o
+
+    def tmn2Deo_or_tmn2Doe_eos(self, par_out: int, inp, anis=None, out=None):
+        """out (parity par_out) = -2 x hopping of inp (the opposite parity)."""
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_hop_eo, lambda i, o: (int(par_out), i, o, a[0], a[1]), inp,
+                           (self.Vh, 4, 3, 2), out)
+
+    def tmDee_or_oo_eos(self, kappa, mu, inp, out=None):
+        return self._unary(self.lib.tms_tmDee, lambda i, o: (kappa, mu, i, o), inp, (self.Vh, 4, 3, 2), out)
+
+    def inv_tmDee_or_oo_eos(self, kappa, mu, inp, out=None):
+        return self._unary(self.lib.tms_inv_tmDee, lambda i, o: (kappa, mu, i, o), inp, (self.Vh, 4, 3, 2), out)
+
+    def tmDkern_eoprec_eos(self, kappa, mu, inp, anis=None, out=None):
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_kern_eoprec, lambda i, o: (kappa, a[0], a[1], mu, i, o), inp,
+                           (self.Vh, 4, 3, 2), out)
+
+    def tmDkern_eoprec_square_eos(self, kappa, mu, inp, anis=None, out=None):
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_kern_eoprec_square, lambda i, o: (kappa, a[0], a[1], mu, i, o), inp,
+                           (self.Vh, 4, 3, 2), out)
+
+    def apply_tmQ(self, kappa, mu, inp, anis=None, out=None):
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_apply_tmQ, lambda i, o: (kappa, a[0], a[1], mu, i, o), inp,
+                           (self.V, 4, 3, 2), out)
+
+    def apply_tmQ2(self, kappa, mu, inp, anis=None, out=None):
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_apply_tmQ2, lambda i, o: (kappa, a[0], a[1], mu, i, o), inp,
+                           (self.V, 4, 3, 2), out)
+
+    # ------------------------------------------------------------ solvers
+    def inv_tmDkern_eoprec_square_eos_cg(self, kappa, mu, source, niter, residue, guess=None, anis=None,
+                                         precision="double", out=None, raise_on_error=True):
+        """Solve K(+mu)K(-mu) sol = source on odd sites.  Returns (sol, stats)."""
+        shape = (self.Vh, 4, 3, 2)
+        s, g = _Buf(source, shape), _Buf(guess, shape)
+        sol = self._new_out(source, shape) if out is None else out
+        o = _Buf(sol, shape, out=True)
+        self._mode(s, g, o)
+        stats = _lib.Stats()
+        a = self._anis(anis)
+        st = self.lib.tms_cg_eoprec_square(self.h, o.ptr, g.ptr, s.ptr, kappa, a[0], a[1], mu, int(niter),
+                                           float(residue), PRECISION[precision], ctypes.byref(stats))
+        if raise_on_error:
+            self._check(st, "inv_tmDkern_eoprec_square_eos_cg", stats.as_dict(), sol)
+        return sol, stats.as_dict()
+
+    def inv_tmD_cg_eoprec(self, kappa, mu, source_lx, niter, residue, anis=None, precision="double", out=None,
+                          raise_on_error=True):
+        """Full solve D_tm sol = source (lx spinors) via e/o preconditioning.  Returns (sol, stats)."""
+        shape = (self.V, 4, 3, 2)
+        s = _Buf(source_lx, shape)
+        sol = self._new_out(source_lx, shape) if out is None else out
+        o = _Buf(sol, shape, out=True)
+        self._mode(s, o)
+        stats = _lib.Stats()
+        a = self._anis(anis)
+        st = self.lib.tms_cg_eoprec(self.h, o.ptr, s.ptr, kappa, a[0], a[1], mu, int(niter), float(residue),
+                                    PRECISION[precision], ctypes.byref(stats))
+        if raise_on_error:
+            self._check(st, "inv_tmD_cg_eoprec", stats.as_dict(), sol)
+        return sol, stats.as_dict()

@@ -1,0 +1,103 @@
+"""CUDA solvers (through the C ABI) against the reference's fixtures and the
+oracle.  FP64 solutions must agree to 1e-9 relative at a 1e-12 target
+(|r|/|b|, i.e. residue 1e-24 in the reference's squared convention); mixed
+precision solutions are reported against the FP64 oracle and must reach the
+target true residual."""
+import numpy as np
+import pytest
+
+import oracle
+from nissa_b200 import Lattice, TmError
+from nissa_b200 import workload as wl
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def test_cg_square_matches_reference_fixture(cuda_device, golden_small):
+    g = golden_small
+    T, L = int(g["T"]), int(g["L"])
+    with Lattice(T, L) as lat:
+        lat.upload_conf(g["conf"])
+        sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(float(g["kappa"]), float(g["mu"]), g["in_odd"], 10000, 1e-24)
+        assert abs(st["iterations"] - int(g["cg_iters"])) <= 1
+        assert rel(sol, g["cg"]) < 1e-9
+        assert st["true_rel_res2"] < 2e-24
+
+
+def test_full_solve_matches_reference_fixture(cuda_device, golden_small):
+    g = golden_small
+    T, L = int(g["T"]), int(g["L"])
+    with Lattice(T, L) as lat:
+        lat.upload_conf(g["conf"])
+        sol, st = lat.inv_tmD_cg_eoprec(float(g["kappa"]), float(g["mu"]), g["in_lx"], 10000, 1e-24)
+        assert abs(st["iterations"] - int(g["cgfull_iters"])) <= 1
+        assert rel(sol, g["cgfull"]) < 1e-9
+        assert st["lx_rel_res2"] < 1e-22
+
+
+def test_config1_plain_fp64_cg(cuda_device, golden_cg):
+    """8^3x16, kappa 0.16, mu 0.01, eps 0.4, point source, |r|/|b| <= 1e-12."""
+    g = golden_cg
+    T, L = int(g["T"]), int(g["L"])
+    conf = wl.gauge_conf(T, L, float(g["eps"]), int(g["seed"]))
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        sol, st = lat.inv_tmD_cg_eoprec(float(g["kappa"]), float(g["mu"]), wl.point_source(T, L), 100000,
+                                        float(g["residue"]))
+        assert abs(st["iterations"] - int(g["iters"])) <= 2
+        assert rel(sol[::8], g["sol_every8"]) < 1e-9
+        assert st["lx_rel_res2"] < 1e-22
+
+
+@pytest.mark.parametrize("precision", ["single", "half"])
+def test_mixed_precision_reaches_target(cuda_device, precision):
+    T, L = 16, 8
+    kappa, mu = 0.1610, 0.005
+    conf = wl.gauge_conf(T, L, 0.35, seed=21)
+    geo = oracle.Geom(T, L)
+    ceo = geo.split(wl.apply_time_bc(conf, T, L))
+    src = wl.random_spinor(geo.Vh, 9)
+    ref, _, _ = geo.cg_eos(ceo, kappa, mu, src, 100000, 1e-26)
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(kappa, mu, src, 100000, 1e-20, precision=precision)
+        assert st["true_rel_res2"] < 1e-20
+        assert st["reliable_updates"] >= 1
+        err = rel(sol, ref)
+        assert err < 1e-8, err
+
+
+def test_guess_is_used(cuda_device, golden_small):
+    g = golden_small
+    T, L = int(g["T"]), int(g["L"])
+    with Lattice(T, L) as lat:
+        lat.upload_conf(g["conf"])
+        sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(float(g["kappa"]), float(g["mu"]), g["in_odd"], 10000, 1e-24,
+                                                       guess=g["cg"])
+        assert st["iterations"] <= 2
+        assert rel(sol, g["cg"]) < 1e-9
+
+
+def test_solver_error_paths(cuda_device):
+    T, L = 4, 4
+    with Lattice(T, L) as lat:
+        lat.upload_conf(wl.gauge_conf(T, L, 0.4, 2))
+        z = np.zeros((lat.Vh, 4, 3, 2))
+        with pytest.raises(TmError) as e:
+            lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, z, 100, 1e-20)
+        assert e.value.status == 8  # invalid source norm
+        x = wl.random_spinor(lat.Vh, 1)
+        with pytest.raises(TmError) as e:
+            lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, x, 3, 1e-24)
+        assert e.value.status == 1  # not converged
+        assert e.value.stats["iterations"] >= 3
+        xn = x.copy()
+        xn[3, 1, 2, 0] = np.nan
+        with pytest.raises(TmError) as e:
+            lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, xn, 100, 1e-20)
+        assert e.value.status in (2, 8)
+        for prec in ("single", "half"):
+            with pytest.raises(TmError) as e:
+                lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, x, 3, 1e-24, precision=prec)
+            assert e.value.status == 1
