@@ -1,0 +1,370 @@
+"""Benchmark: twisted-mass e/o CG solves per second on one B200 (or N replicas).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one full solve D_tm psi = eta through the e/o
+preconditioned CG, the reference's inv_tmD_cg_eoprec): 32^3 x 64 lattice,
+gauge links U = exp(i eps H) with eps = 0.35 (seeded), antiperiodic time,
+kappa = 0.1610, mu = 0.005, point sources at the origin cycling over the 12
+spin-colour columns, stopped at |r|/|b| <= 1e-10 (squared residue 1e-20), in
+mixed precision: FP32 inner CG with 12-real links and FP64 reliable updates.
+
+Printed JSON line (rank 0): value = solves/s with the inputs resident in HBM
+(device timing, CUDA events, max over ranks); e2e = the same through the C
+ABI with host (pinned) buffers, host<->device copies inside the timed region;
+roofline = the inner solver's hopping kernel (FP32, 12-real links) timed alone
+with CUDA events, L2 flushed between launches; fp64 = the plain FP64 GPU CG on
+the same solves and the FP64 e/o Dslash bandwidth; cpu_baseline = the
+reference's own OpenMP CG (oracle/_ref) on a bounded sample of the same solve.
+
+N > 1 GPUs run independent replicas (one gauge copy per GPU, each rank solving
+its own columns): the path needs no collective, scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="tm e/o CG solve, 32^3x64, mixed FP32-inner/FP64-reliable, |r|/|b|<=1e-10",
+                T=64, L=32, eps=0.35, seed=1, kappa=0.1610, mu=0.005, residue=1e-20, bc_t=-1.0)
+METRIC = "CG solves/s & Dslash HBM GB/s, 32³×64 mixed vs FP64 @1e-10; p50/p99 serve"
+UNIT = "solves/s"
+CPU_SAMPLE_ITERS = 20
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        except Exception:
+            rows = []
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        loaded = [s for s in sm if smax and s > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference_sample(conf_bc, T, L, kappa, mu, iters, threads):
+    """The reference's own CG (oracle/_ref) for `iters` iterations on the host:
+    seconds per iteration.  Falls back to the oracle restatement if the
+    reference build is absent."""
+    import oracle
+    Vh = T * L ** 3 // 2
+    src = np.random.default_rng(5).standard_normal((Vh, 4, 3, 2))
+    if oracle.ref_available():
+        _, rec, _ = oracle.run_ref("cg", T, L, {"conf": conf_bc, "in": src}, None, kappa=kappa, mu=mu,
+                                   sample_iters=iters, threads=threads)
+        # the reference runs `iters` iterations plus one final residual operator application
+        return rec["seconds"] / (iters + 1), "reference", rec.get("threads", threads)
+    geo = oracle.Geom(T, L)
+    ceo = geo.split(conf_bc)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    t0 = time.perf_counter()
+    geo.cg_eos(ceo, kappa, mu, src, iters, 1e-300)
+    return (time.perf_counter() - t0) / (iters + 1), "port", threads
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference's own OpenMP CG on the host cores, on a
+    bounded sample of each solve, scaled to solves/s by the FP64 iteration
+    count of the full solve."""
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from nissa_b200 import workload as wl
+    W = WORKLOAD
+    T, L = W["T"], W["L"]
+    threads = os.cpu_count() or 1
+    conf = wl.apply_time_bc(wl.gauge_conf(T, L, W["eps"], W["seed"]), T, L, W["bc_t"])
+    iters_full = args.fp64_iters
+    vals = []
+    for s in range(args.warmup + args.steps):
+        spi, kind, cores = cpu_reference_sample(conf, T, L, W["kappa"], W["mu"], CPU_SAMPLE_ITERS, threads)
+        if s >= args.warmup:
+            vals.append(1.0 / (spi * iters_full))
+    v = statistics.median(vals)
+    sample = ("inv_tmDkern_eoprec_square_eos_cg on %d^3x%d for %d iterations (+1 final residual) per step, "
+              "scaled by %d FP64 CG iterations per full solve" % (L, T, CPU_SAMPLE_ITERS, iters_full))
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic (seeded gauge recipe)",
+                      "config": {"workload": W["name"].replace("mixed FP32-inner/FP64-reliable", "FP64 CPU"),
+                                 "T": T, "L": L, "kappa": W["kappa"], "mu": W["mu"], "eps": W["eps"],
+                                 "residue": W["residue"]},
+                      "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+                      "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from nissa_b200 import Lattice
+    from nissa_b200 import workload as wl
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = "cuda:%d" % local
+    if ws > 1:
+        dist.init_process_group("nccl", device_id=torch.device(dev), timeout=__import__("datetime").timedelta(
+            seconds=600))
+    W = WORKLOAD
+    T, L = W["T"], W["L"]
+    V = T * L ** 3
+    kappa, mu, residue = W["kappa"], W["mu"], W["residue"]
+
+    t0 = time.perf_counter()
+    conf = wl.gauge_conf(T, L, W["eps"], W["seed"], device=dev)
+    log("rank %d: gauge conf %.1fs" % (rank, time.perf_counter() - t0))
+    lat = Lattice(T, L, bc_t=W["bc_t"], device=local)
+    lat.upload_conf(conf)
+    assert lat.conf_is_su3
+
+    def column(k):
+        s = torch.zeros((V, 4, 3, 2), dtype=torch.float64, device=dev)
+        s[0, (k // 3) % 4, k % 3, 0] = 1.0
+        return s
+
+    ncol = min(12, args.steps)
+    cols = [column((rank * args.steps + k) % 12) for k in range(ncol)]
+    sol = torch.empty((V, 4, 3, 2), dtype=torch.float64, device=dev)
+
+    def solve(k, precision="single", src=None, out=None):
+        s = cols[k % ncol] if src is None else src
+        return lat.inv_tmD_cg_eoprec(kappa, mu, s, 100000, residue, precision=precision,
+                                     out=sol if out is None else out)[1]
+
+    for k in range(args.warmup):
+        solve(k)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # --- timed region: device-resident inputs -------------------------------------------
+    stats = []
+    barrier()
+    l0 = lat.launch_count
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(args.steps):
+            stats.append(solve(k))
+        e1.record()
+        barrier()
+    launches = lat.launch_count - l0
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = ws * args.steps / (ms_max * 1e-3)
+    clocks = clk.summary()
+
+    # --- e2e: same solves through the C ABI with pinned host buffers -----------------------
+    host_src = [torch.zeros((V, 4, 3, 2), dtype=torch.float64).pin_memory() for _ in range(ncol)]
+    for k in range(ncol):
+        host_src[k].copy_(cols[k].cpu())
+    host_sol = torch.empty((V, 4, 3, 2), dtype=torch.float64).pin_memory()
+    solve(0, src=host_src[0], out=host_sol)  # warm the host path
+    e2e_steps = max(1, min(args.steps, 4))
+    barrier()
+    h0 = time.perf_counter()
+    for k in range(e2e_steps):
+        solve(k, src=host_src[k % ncol], out=host_sol)
+    barrier()
+    e2e_s = time.perf_counter() - h0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = ws * e2e_steps / float(t.item())
+    bytes_per = V * 24 * 8
+
+    # --- plain FP64 GPU CG on the same solves, and the accuracy of the mixed solutions -------
+    fp64_steps = 2
+    fp64_stats, errs = [], []
+    ref = torch.empty_like(sol)
+    torch.cuda.synchronize()
+    f0 = time.perf_counter()
+    for k in range(fp64_steps):
+        fp64_stats.append(solve(k, precision="double", out=ref))
+        solve(k, precision="single", out=sol)
+        errs.append(float(torch.linalg.norm(sol - ref) / torch.linalg.norm(ref)))
+    fp64_sec = statistics.mean(s["seconds"] for s in fp64_stats)
+    mixed_sec = statistics.mean(s["seconds"] for s in stats)
+
+    # --- roofline: the inner solver's hopping kernel, and the FP64 Dslash -------------------
+    peak, peak_kind = peaks()
+    hop_ms, hop_bytes = lat.bench_hop("single", variant=1, nrep=30, flush=True)
+    d64_ms, d64_bytes = lat.bench_hop("double", variant=0, nrep=30, flush=True)
+    achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
+    d64_gbs = d64_bytes / (d64_ms * 1e-3) / 1e9
+
+    # --- CPU baseline: the reference's own CG on a bounded sample (rank 0, N=1 only) ---------
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            conf_bc = wl.apply_time_bc(conf, T, L, W["bc_t"])
+            spi, kind, cores = cpu_reference_sample(conf_bc, T, L, kappa, mu, CPU_SAMPLE_ITERS, os.cpu_count() or 1)
+            it64 = fp64_stats[0]["iterations"]
+            cpu = {"value": 1.0 / (spi * it64), "unit": UNIT, "cores": cores, "kind": kind,
+                   "sample": "reference inv_tmDkern_eoprec_square_eos_cg, %d iterations (+1 final residual) on the "
+                             "same 32^3x64 conf, %.3f s/iteration, scaled by the %d FP64 iterations of a full solve"
+                             % (CPU_SAMPLE_ITERS, spi, it64)}
+        except Exception as e:  # the CPU baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable", "sample": str(e)}
+
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 inner / f64 reliable updates",
+        "data": "synthetic (seeded gauge recipe U=exp(i eps H), point sources)",
+        "config": {"workload": W["name"], "T": T, "L": L, "kappa": kappa, "mu": mu, "eps": W["eps"],
+                   "residue_sq": residue, "sources": "12 point spin-colour columns at the origin, cycled",
+                   "l2": "working set (links 0.4 GB FP32 + spinors) larger than the 126 MB L2",
+                   "parallelism": "replicas" if ws > 1 else "1 GPU"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_per, "d2h_bytes_per_step": bytes_per,
+                "steps": e2e_steps},
+        "roofline": {"bound": "hbm", "kernel": "hop_kernel<FP32, 12-real links> + inverse diagonal (CG first half)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "ms_per_launch": hop_ms,
+                     "alg_bytes_per_launch": hop_bytes},
+        "fp64": {"solves_per_s": 1.0 / fp64_sec, "iterations": fp64_stats[0]["iterations"],
+                 "mixed_speedup_vs_fp64": fp64_sec / mixed_sec,
+                 "dslash_gbs": d64_gbs, "dslash_frac": d64_gbs / peak, "dslash_ms": d64_ms},
+        "accuracy": {"mixed_rel_err_vs_fp64": max(errs),
+                     "true_rel_res2_max": max(s["true_rel_res2"] for s in stats),
+                     "lx_rel_res2_max": max(s["lx_rel_res2"] for s in stats)},
+        "solver": {"iterations_mean": statistics.mean(s["iterations"] for s in stats),
+                   "reliable_updates_mean": statistics.mean(s["reliable_updates"] for s in stats)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_kernel_only(args):
+    """Profiling entry point: set up the workload's lattice and launch the e/o
+    hopping kernel of one precision `nrep` times (L2 flushed between launches)."""
+    import torch
+    from nissa_b200 import Lattice
+    from nissa_b200 import workload as wl
+    W = WORKLOAD
+    conf = wl.gauge_conf(W["T"], W["L"], W["eps"], W["seed"], device="cuda:0")
+    lat = Lattice(W["T"], W["L"], bc_t=W["bc_t"])
+    lat.upload_conf(conf)
+    ms, by = lat.bench_hop(args.kernel_only, variant=args.variant, nrep=args.nrep, flush=True)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel": "hop", "precision": args.kernel_only, "variant": args.variant, "T": W["T"],
+                      "L": W["L"], "ms_per_launch": ms, "alg_bytes_per_launch": by,
+                      "achieved_gbs": by / (ms * 1e-3) / 1e9}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--fp64-iters", type=int, default=FP64_ITERS,
+                    help="FP64 CG iterations of one full solve (scales the reference arm's bounded sample)")
+    ap.add_argument("--lattice", default=None, help="T,L override for quick checks (not the benchmark workload)")
+    ap.add_argument("--kernel-only", default=None, choices=["double", "single", "half"],
+                    help="only time the e/o hopping kernel of this precision (profiling entry point)")
+    ap.add_argument("--variant", type=int, default=1, help="hopping kernel variant for --kernel-only")
+    ap.add_argument("--nrep", type=int, default=10, help="launches for --kernel-only")
+    args = ap.parse_args()
+    if args.lattice:
+        T, L = (int(x) for x in args.lattice.split(","))
+        WORKLOAD.update(T=T, L=L, name=WORKLOAD["name"].replace("32^3x64", "%d^3x%d" % (L, T)))
+    if args.kernel_only:
+        run_kernel_only(args)
+        return
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+# FP64 CG iterations of one full solve of this workload (measured on the GPU's
+# plain FP64 CG, which matches the reference's iteration count; printed by each
+# run of this script under "fp64.iterations").
+FP64_ITERS = 1000
+
+if __name__ == "__main__":
+    main()

@@ -131,6 +131,19 @@ tms_status tms_cg_eoprec_square(tms_ctx *ctx, double *sol, const double *guess, 
 tms_status tms_cg_eoprec(tms_ctx *ctx, double *sol_lx, const double *src_lx, double kappa, int has_anis,
                          double anis, double mu, int niter, double residue, int precision, tms_stats *stats);
 
+/* ---- instrumentation (no reference counterpart) ---- */
+
+/* Number of CUDA kernels this context has launched (CUDA-graph replays count their nodes). */
+uint64_t tms_launch_count(const tms_ctx *ctx);
+/* Time the e/o hopping kernel alone with CUDA events on the context's stream: nrep launches,
+ * each preceded (untimed) by a 512 MiB write that flushes the L2 when flush=1.
+ * precision: tms_precision; variant 0 plain hop, 1 hop + inverse diagonal (CG first half),
+ * 2 hop + diagonal + gamma5 combine + |out|^2 reduction (CG second half).
+ * Outputs the mean device time per launch and the algorithmic (compulsory) bytes per launch:
+ * Vh x (8 links + input spinor + output spinor [+ own-site spinor for variant 2]). */
+tms_status tms_bench_hop(tms_ctx *ctx, int precision, int variant, int nrep, int flush, double *ms_per_launch,
+                         double *bytes_per_launch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,6 +80,10 @@ struct tms_ctx
   // CUDA graphs of one CG iteration block, per precision (0: FP64, 1: FP32, 2: FP16)
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int graph_iters = 8;
+  uint64_t graph_nodes[3] = {0, 0, 0};
+
+  // kernels launched by this context (graph replays count their nodes)
+  uint64_t launches = 0;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -168,6 +172,7 @@ namespace
                   const int* stop = nullptr)
   {
     const int nsite = (int)(npar * c->g.Vh);
+    ++c->launches;
     hop_kernel<P, LF, Epi, Fin><<<div_up(nsite, HOP_THREADS), HOP_THREADS, 0, s>>>(
       c->g, par_out, npar, view<P>(in_e), view<P>(in_o), U, prm, epi, reducer(c), fin, stop);
   }
@@ -326,6 +331,7 @@ namespace
         d = ctx->stage;
       }
     const int n = (int)ctx->g.Vh;
+    ++ctx->launches;
     aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, d, site_map, view<PREC_F64>(f));
     CU(cudaGetLastError());
     return TMS_OK;
@@ -342,6 +348,7 @@ namespace
         d = ctx->stage;
       }
     const int n = (int)ctx->g.Vh;
+    ++ctx->launches;
     soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, view<PREC_F64>(f), site_map, d);
     CU(cudaGetLastError());
     if (ctx->ptr_mode == TMS_PTR_HOST && flush)
@@ -378,6 +385,7 @@ namespace
   tms_status norm2(tms_ctx* ctx, const Field& a, double* out)
   {
     const int n = (int)ctx->g.Vh;
+    ++ctx->launches;
     norm_kernel<P, false><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, view<P>(a), view<P>(a),
                                                                                       reducer(ctx));
     CU(cudaGetLastError());
@@ -405,6 +413,7 @@ namespace
     kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
     kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
     const int n = (int)ctx->g.Vh;
+    ++ctx->launches;
     residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
       n, view<PREC_F64>(b), view<PREC_F64>(s), view<PREC_F64>(r), reducer(ctx));
     CU(cudaGetLastError());
@@ -431,6 +440,7 @@ namespace
         EpiKernCgUpdate<P, PX> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), prm, c->st, +1.0};
         launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
         const int n = (int)c->g.Vh;
+        ++c->launches;
         xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s>>>(n, view<P>(r), view<P>(p), c->st, stop);
       }
   }
@@ -443,7 +453,10 @@ namespace
     CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t graph;
     CU(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = ctx->launches;
     record_cg_iterations<P, PX, LF>(ctx, cs, U, v, x, ctx->graph_iters);
+    ctx->graph_nodes[slot] = ctx->launches - before;
+    ctx->launches = before;
     cudaError_t e = cudaStreamEndCapture(cs, &graph);
     cudaStreamDestroy(cs);
     if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
@@ -469,6 +482,7 @@ namespace
   void convert(tms_ctx* c, const Field& src, const Field& dst, double a = 1.0)
   {
     const int n = (int)c->g.Vh;
+    ++c->launches;
     axpby_kernel<PD, PS, PS><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, c->stream>>>(n, a, view<PS>(src), 0.0,
                                                                                        view<PS>(src), view<PD>(dst));
   }
@@ -509,6 +523,7 @@ namespace
     while (S.stop == STOP_RUN)
       {
         CU(cudaGraphLaunch(ctx->graph[0], ctx->stream));
+        ctx->launches += ctx->graph_nodes[0];
         TRY(pull_state(ctx));
       }
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -546,6 +561,14 @@ namespace
     for (int i = 1; i <= 6; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
     if (ctx->lo_prec != P)
       {
+        // the inner-precision fields move: graphs captured on the old ones are void
+        CU(cudaStreamSynchronize(ctx->stream));
+        for (int g = 1; g < 3; g++)
+          if (ctx->graph[g])
+            {
+              cudaGraphExecDestroy(ctx->graph[g]);
+              ctx->graph[g] = nullptr;
+            }
         for (auto& l : ctx->lo) TRY(alloc_field(ctx, l, P));
         ctx->lo_prec = P;
       }
@@ -588,6 +611,7 @@ namespace
         for (;;)
           {
             CU(cudaGraphLaunch(ctx->graph[slot], ctx->stream));
+            ctx->launches += ctx->graph_nodes[slot];
             TRY(pull_state(ctx));
             if (S.stop == STOP_RUN) continue;
             if (S.stop == STOP_BREAKDOWN)
@@ -597,6 +621,7 @@ namespace
               }
             // reliable update: x += x_lo (FP64), r = b - A x (FP64)
             const int n = (int)ctx->g.Vh;
+            ++ctx->launches;
             axpby_kernel<PREC_F64, PREC_F64, PX><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
               n, 1.0, view<PREC_F64>(f[1]), 1.0, view<PX>(xlo), view<PREC_F64>(f[1]));
             CU(cudaMemsetAsync(xlo.d, 0, xlo.bytes, ctx->stream));
@@ -618,6 +643,7 @@ namespace
             S.rel_trigger = delta * delta * rt;
             S.stop = STOP_RUN;
             TRY(push_state(ctx));
+            ++ctx->launches;
             xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, view<P>(lo[1]),
                                                                                        view<P>(lo[2]), ctx->st,
                                                                                        nullptr);
@@ -651,6 +677,74 @@ namespace
       return ctx->su3 ? cg_mixed<PREC_F16>(ctx, links32r(ctx), 2, niter, residue, have_guess, stats)
                       : cg_mixed<PREC_F16>(ctx, links32f(ctx), 2, niter, residue, have_guess, stats);
     return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
+  }
+}
+
+namespace
+{
+  template <int P, int LF>
+  tms_status bench_hop_t(tms_ctx* ctx, const LinkT<LF>& U, int variant, int nrep, int flush, double* ms,
+                         double link_bytes, double spinor_bytes, double* bytes)
+  {
+    Field in, out, x;
+    TRY(alloc_field(ctx, in, P));
+    TRY(alloc_field(ctx, out, P));
+    TRY(alloc_field(ctx, x, P));
+    struct G
+    {
+      Field *a, *b, *c;
+      ~G()
+      {
+        for (Field* f : {a, b, c})
+          {
+            if (f->d) cudaFree(f->d);
+            if (f->n) cudaFree(f->n);
+          }
+      }
+    } guard{&in, &out, &x};
+    // deterministic non-trivial input: the ones vector scaled
+    const int n = (int)ctx->g.Vh;
+    axpby_kernel<P, P, P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, 0.0, view<P>(in), 0.0,
+                                                                                     view<P>(in), view<P>(in));
+    void* scratch = nullptr;
+    const size_t sbytes = size_t(512) << 20;
+    if (flush) CU(cudaMalloc(&scratch, sbytes));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double total = 0;
+    for (int r = 0; r < nrep; r++)
+      {
+        if (flush) cudaMemsetAsync(scratch, r & 0xff, sbytes, ctx->stream);
+        cudaEventRecord(e0, ctx->stream);
+        if (variant == 0)
+          {
+            EpiPlain<P> e{{view<P>(out), view<P>(out)}};
+            launch_hop<P, LF>(ctx, ctx->stream, 0, 1, in, in, U, ctx->prm, e);
+          }
+        else if (variant == 1)
+          {
+            EpiInvDiag<P> e{{view<P>(out), view<P>(out)}, ctx->prm, 1.0};
+            launch_hop<P, LF>(ctx, ctx->stream, 0, 1, in, in, U, ctx->prm, e);
+          }
+        else
+          {
+            EpiKern<P, true> e{{view<P>(out), view<P>(out)}, {view<P>(x), view<P>(x)}, ctx->prm, 1.0};
+            launch_hop<P, LF>(ctx, ctx->stream, 1, 1, in, in, U, ctx->prm, e);
+          }
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        total += t;
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (scratch) cudaFree(scratch);
+    CU(cudaGetLastError());
+    *ms = total / nrep;
+    *bytes = (double)ctx->g.Vh * (8 * link_bytes + 2 * spinor_bytes + (variant == 2 ? spinor_bytes : 0));
+    return TMS_OK;
   }
 }
 
@@ -695,6 +789,7 @@ tms_status tms_create4(tms_ctx** out, int T, int LX, int LY, int LZ, double bc_t
   cudaMemset(ctx->st, 0, sizeof(CgState));
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
+  ++ctx->launches;
   lx_of_eo_kernel<<<div_up(V, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->lx_of_eo);
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
     return cleanup(TMS_ERR_CUDA);
@@ -760,6 +855,7 @@ tms_status tms_geometry_tables(tms_ctx* ctx, int32_t* parity, int32_t* eo_of_lx,
   const int64_t V = ctx->g.V;
   int* d = nullptr;
   CU(cudaMalloc(&d, sizeof(int) * V * 11));
+  ++ctx->launches;
   geometry_tables_kernel<<<div_up(V, 256), 256, 0, ctx->stream>>>(ctx->g, d, d + V, d + 2 * V, d + 3 * V, d + 7 * V);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -789,9 +885,11 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
       src = ctx->stage;
     }
   const int unfold = (flags & TMS_CONF_BC_INCLUDED) ? 1 : 0;
+  ++ctx->launches;
   conf_to_soa_kernel<<<div_up(V, 128), 128, 0, ctx->stream>>>(ctx->g, src, layout, unfold, ctx->lx_of_eo, ctx->U64);
   CU(cudaGetLastError());
   const int64_t nl = 8 * Vh;
+  ++ctx->launches;
   conf_lowprec_kernel<<<div_up(nl, 256), 256, 0, ctx->stream>>>(nl, (int)Vh, ctx->U64, ctx->U32r, ctx->U32f,
                                                                  reducer(ctx));
   CU(cudaGetLastError());
@@ -828,6 +926,7 @@ static tms_status diag_common(tms_ctx* ctx, double kappa, double mu, const doubl
   TRY(spinor_in(ctx, in, nullptr, ctx->g.Vh, a));
   TRY(alloc_field(ctx, b, PREC_F64));
   const int n = (int)ctx->g.Vh;
+  ++ctx->launches;
   diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, view<PREC_F64>(a), view<PREC_F64>(b), ctx->prm,
                                                                    1.0, inverse);
   CU(cudaGetLastError());
@@ -897,7 +996,9 @@ static tms_status tmQ_common(tms_ctx* ctx, double kappa, int has_anis, double an
       src = ctx->stage;
     }
   const int n = (int)Vh;
+  ++ctx->launches;
   aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, view<PREC_F64>(f[6]));
+  ++ctx->launches;
   aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh,
                                                                        view<PREC_F64>(f[7]));
   auto U = links64(ctx);
@@ -919,6 +1020,7 @@ static tms_status tmQ_common(tms_ctx* ctx, double kappa, int has_anis, double an
   TRY(spinor_out(ctx, f[4], ctx->lx_of_eo, ctx->g.V, out, false));
   // second parity goes to the same staging/destination buffer
   double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : out;
+  ++ctx->launches;
   soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(5), ctx->lx_of_eo + Vh, d);
   CU(cudaGetLastError());
   if (ctx->ptr_mode == TMS_PTR_HOST)
@@ -977,9 +1079,12 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
       CU(cudaMemcpyAsync(ctx->stage, src_lx, bytes, cudaMemcpyHostToDevice, ctx->stream));
       src = ctx->stage;
     }
+  ++ctx->launches;
   aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(eta[0]));
+  ++ctx->launches;
   aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
   // Eq. (8a): te = D_ee^-1 eta_e ; Eq. (8b): varphi = g5 (eta_o + hop(te)/2) -> f0
+  ++ctx->launches;
   diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(eta[0]), V(f[5]), ctx->prm, 1.0, 1);
   EpiSrcPrep<PREC_F64> sp{{V(f[0]), V(f[0])}, {V(eta[1]), V(eta[1])}};
   launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
@@ -994,7 +1099,9 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
   CU(cudaGetLastError());
   // paste_eo_parts_into_lx_vector
   double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sol_lx;
+  ++ctx->launches;
   soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, d);
+  ++ctx->launches;
   soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, d);
   CU(cudaGetLastError());
   if (ctx->ptr_mode == TMS_PTR_HOST) CU(cudaMemcpyAsync(sol_lx, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1006,6 +1113,7 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
       double num = 0, den = 0;
       for (int par = 0; par < 2; par++)
         {
+          ++ctx->launches;
           g5_residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, V(f[2 + par]), V(eta[par]),
                                                                                        reducer(ctx));
           CU(cudaGetLastError());
@@ -1018,6 +1126,31 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
     }
   TRY(finish(ctx));
   return st;
+}
+
+uint64_t tms_launch_count(const tms_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+tms_status tms_bench_hop(tms_ctx* ctx, int precision, int variant, int nrep, int flush, double* ms_per_launch,
+                         double* bytes_per_launch)
+{
+  TRY(check_conf(ctx));
+  if (nrep <= 0 || variant < 0 || variant > 2 || !ms_per_launch || !bytes_per_launch)
+    return fail(ctx, TMS_ERR_BAD_ARG, "bad bench arguments");
+  TRY(set_params(ctx, 0.16, 0.01, 0, 1.0));
+  if (precision == TMS_PREC_DOUBLE)
+    return bench_hop_t<PREC_F64>(ctx, links64(ctx), variant, nrep, flush, ms_per_launch, 144.0, 192.0,
+                                 bytes_per_launch);
+  if (precision == TMS_PREC_MIXED_SINGLE)
+    return ctx->su3 ? bench_hop_t<PREC_F32>(ctx, links32r(ctx), variant, nrep, flush, ms_per_launch, 48.0, 96.0,
+                                            bytes_per_launch)
+                    : bench_hop_t<PREC_F32>(ctx, links32f(ctx), variant, nrep, flush, ms_per_launch, 72.0, 96.0,
+                                            bytes_per_launch);
+  if (precision == TMS_PREC_MIXED_HALF)
+    return ctx->su3 ? bench_hop_t<PREC_F16>(ctx, links32r(ctx), variant, nrep, flush, ms_per_launch, 48.0, 52.0,
+                                            bytes_per_launch)
+                    : bench_hop_t<PREC_F16>(ctx, links32f(ctx), variant, nrep, flush, ms_per_launch, 72.0, 52.0,
+                                            bytes_per_launch);
+  return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
 }
 
 } // extern "C"

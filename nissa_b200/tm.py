@@ -195,6 +195,20 @@ class Lattice:
         return self._unary(self.lib.tms_apply_tmQ2, lambda i, o: (kappa, a[0], a[1], mu, i, o), inp,
                            (self.V, 4, 3, 2), out)
 
+    # ---------------------------------------------------- instrumentation
+    @property
+    def launch_count(self) -> int:
+        """CUDA kernels launched by this lattice's context so far."""
+        return int(self.lib.tms_launch_count(self.h))
+
+    def bench_hop(self, precision="double", variant=0, nrep=20, flush=True):
+        """Mean device time (ms) of one e/o hopping launch and its algorithmic bytes."""
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        st = self.lib.tms_bench_hop(self.h, PRECISION[precision], int(variant), int(nrep), 1 if flush else 0,
+                                    ctypes.byref(ms), ctypes.byref(by))
+        self._check(st, "tms_bench_hop")
+        return ms.value, by.value
+
     # ------------------------------------------------------------ solvers
     def inv_tmDkern_eoprec_square_eos_cg(self, kappa, mu, source, niter, residue, guess=None, anis=None,
                                          precision="double", out=None, raise_on_error=True):

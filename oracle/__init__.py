@@ -249,9 +249,13 @@ def run_ref(op: str, T: int, L: int, arrays: dict, out_shape, threads: int | Non
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
         cp = subprocess.run(argv, cwd=d, env=env, capture_output=True, text=True)
-        if cp.returncode != 0:
+        recs = [l for l in cp.stdout.splitlines() if l.startswith('{"op"')]
+        if cp.returncode != 0 or not recs:
             raise RuntimeError("nissa_ref %s failed (%d): %s" % (op, cp.returncode, (cp.stdout + cp.stderr)[-2000:]))
-        rec = json.loads(cp.stdout.strip().splitlines()[-1])
+        rec = json.loads(recs[-1])
+        if "sample_iters" in params:
+            # bounded sample: the reference ended through its non-convergence path
+            return None, rec, cp.stdout
         out = None
         if out_shape is not None and os.path.exists(out_path):
             out = np.fromfile(out_path, np.float64).reshape(out_shape)

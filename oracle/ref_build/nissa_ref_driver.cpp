@@ -23,6 +23,12 @@
 //        cgm conf in out kappa masses=a,b residues=a,b niter
 //                                                inv_tmclovQ2_cgm with a zero clover term (cgm_invert_tmclovQ2.cpp:10-32)
 //   common keys: anis=<double> (default: none), reps=<n> (timed repetitions, default 1)
+//   cg with sample_iters=N: a bounded sample of the solve.  The reference's CG
+//   runs exactly N iterations (niter=N, unreachable residue) plus its final
+//   true-residual application, then takes its own non-convergence path
+//   (CRASH, cg_invert_template_threaded.hpp:146-147); the driver reports the
+//   elapsed time from the reference's crash hook (base/debug.hpp:70) and the
+//   process exits through the single-rank MPI_Abort.
 // The last stdout line is a JSON record with the time per repetition.
 
 #include <config.hpp>
@@ -154,6 +160,17 @@ namespace
   double now()
   {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  }
+
+  double sample_t0 = 0;
+  int sample_iters = 0;
+  int sample_T = 0, sample_L = 0;
+
+  void sample_report()
+  {
+    printf("{\"op\": \"cg\", \"T\": %d, \"L\": %d, \"sample_iters\": %d, \"threads\": %d, \"seconds\": %.9g}\n",
+	   sample_T, sample_L, sample_iters, omp_get_max_threads(), now() - sample_t0);
+    fflush(stdout);
   }
 }
 
@@ -302,6 +319,17 @@ int main(int narg, char** arg_v)
 		  const double t0 = now();
 		  for (int r = 0; r < reps; r++) tmDkern_eoprec_square_eos(out, temp1, temp2, conf, kappa, anis, mu, in);
 		  t_per_rep = (now() - t0) / reps;
+		}
+	      else if (op == "cg" && args.count("sample_iters"))
+		{
+		  sample_iters = (int)argd("sample_iters");
+		  sample_T = T;
+		  sample_L = L;
+		  crashHook = sample_report;
+		  sample_t0 = now();
+		  inv_tmDkern_eoprec_square_eos_cg(out, std::nullopt, conf, kappa, anis, mu, sample_iters, 1e-300, in);
+		  fprintf(stderr, "sample run converged before %d iterations\n", sample_iters);
+		  return 4;
 		}
 	      else if (op == "cg")
 		{

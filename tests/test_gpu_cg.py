@@ -101,3 +101,23 @@ def test_solver_error_paths(cuda_device):
             with pytest.raises(TmError) as e:
                 lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, x, 3, 1e-24, precision=prec)
             assert e.value.status == 1
+
+
+def test_precision_switching_same_lattice(cuda_device):
+    """single -> half -> single -> double on one context: graphs are rebuilt
+    when the inner fields change precision."""
+    T, L = 8, 4
+    conf = wl.gauge_conf(T, L, 0.35, seed=4)
+    src = wl.random_spinor(T * L ** 3 // 2, 5)
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        sols = []
+        for prec in ("single", "half", "single", "double"):
+            sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, src, 10000, 1e-20, precision=prec)
+            assert st["true_rel_res2"] < 1e-20
+            sols.append(sol)
+        for s in sols[:3]:
+            assert rel(s, sols[3]) < 1e-8
+        n0 = lat.launch_count
+        lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, src, 10000, 1e-20, precision="single")
+        assert lat.launch_count - n0 >= 5 * 10
