@@ -144,6 +144,34 @@ uint64_t tms_launch_count(const tms_ctx *ctx);
 tms_status tms_bench_hop(tms_ctx *ctx, int precision, int variant, int nrep, int flush, double *ms_per_launch,
                          double *bytes_per_launch);
 
+/* ---- allocation-free hopping (no counterpart in the reference) ---- */
+
+/* Lattices of at most this many sites are accepted by tms_hop_eo_noalloc. */
+#define TMS_NOALLOC_MAX_SITES 16384
+
+/* The e/o hopping of tms_hop_eo for callers that cannot let a library allocate
+ * device memory (an application whose own pool owns all device memory, or a
+ * phase where cudaMalloc/cudaFree would synchronise the device).  Needs no
+ * context: the caller passes the gauge configuration each call, like the
+ * reference's operators, and all buffers are DEVICE pointers in the layouts
+ * above (conf: layout TMS_LAYOUT_LX or TMS_LAYOUT_EO, flags as for
+ * tms_conf_upload; in/out: Vh e/o spinors).  Runs on the caller's current
+ * device and on `stream` (NULL: the legacy default stream), and returns after
+ * the stream has finished the work.
+ *
+ * It calls no cudaMalloc/cudaFree and no allocating library routine: its
+ * scratch is one fixed device array of TMS_NOALLOC_MAX_SITES*768+256 bytes
+ * (12 MiB) that every GPU loading this library holds until the process exits.
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current; make that first call before
+ * any stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  Lattices larger than
+ * TMS_NOALLOC_MAX_SITES are rejected with TMS_ERR_BAD_ARG; `err` (may be NULL)
+ * receives a message of at most errlen bytes. */
+tms_status tms_hop_eo_noalloc(int T, int L, double bc_t, const double *conf, int layout, int flags, int par_out,
+                              const double *in, double *out, int has_anis, double anis, void *stream, char *err,
+                              int errlen);
+
 #ifdef __cplusplus
 }
 #endif

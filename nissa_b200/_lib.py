@@ -44,6 +44,7 @@ SIGNATURES = {
     "tms_cg_eoprec": (I, [P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_launch_count": (ctypes.c_uint64, [P]),
     "tms_bench_hop": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),
+    "tms_hop_eo_noalloc": (I, [I, I, D, P, I, I, I, P, P, I, D, P, ctypes.c_char_p, I]),
 }
 
 

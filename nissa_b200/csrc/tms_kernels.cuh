@@ -515,7 +515,7 @@ namespace tms
 
   // p = r + beta p  (cg_invert_template_threaded.hpp:115-124)
   template <int P>
-  __global__ void __launch_bounds__(BLAS_THREADS)
+  static __global__ void __launch_bounds__(BLAS_THREADS)
     xpay_kernel(int n, SpinorT<P> r, SpinorT<P> p, const CgState* st, const int* __restrict__ stop)
   {
     using R = typename SpinorT<P>::R;
@@ -533,7 +533,7 @@ namespace tms
 
   // generic: reduce |a|^2 (or Re(a,b)) over n sites
   template <int P, bool DOT>
-  __global__ void __launch_bounds__(BLAS_THREADS)
+  static __global__ void __launch_bounds__(BLAS_THREADS)
     norm_kernel(int n, SpinorT<P> a, SpinorT<P> b, Reducer red)
   {
     using R = typename SpinorT<P>::R;
@@ -559,7 +559,7 @@ namespace tms
 
   // out = a*x + b*y (any precisions)
   template <int PO, int PX, int PY>
-  __global__ void __launch_bounds__(BLAS_THREADS)
+  static __global__ void __launch_bounds__(BLAS_THREADS)
     axpby_kernel(int n, double a, SpinorT<PX> x, double b, SpinorT<PY> y, SpinorT<PO> out)
   {
     using RO = typename SpinorT<PO>::R;
@@ -587,7 +587,7 @@ namespace tms
   }
 
   // r = b - s and reduce |r|^2 (true residual), FP64
-  __global__ void __launch_bounds__(BLAS_THREADS)
+  static __global__ void __launch_bounds__(BLAS_THREADS)
     residual_kernel(int n, SpinorT<PREC_F64> b, SpinorT<PREC_F64> s, SpinorT<PREC_F64> r, Reducer red)
   {
     const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
@@ -609,7 +609,7 @@ namespace tms
   }
 
   // reduce |g5 q - eta|^2 (the lx residual check of cg_invert_tmD_eoprec.cpp:192-212)
-  __global__ void __launch_bounds__(BLAS_THREADS)
+  static __global__ void __launch_bounds__(BLAS_THREADS)
     g5_residual_kernel(int n, SpinorT<PREC_F64> q, SpinorT<PREC_F64> eta, Reducer red)
   {
     const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
