@@ -334,6 +334,50 @@ def run_kernel_only(args):
                       "achieved_gbs": by / (ms * 1e-3) / 1e9}), flush=True)
 
 
+CGM_WORKLOAD = dict(name="tm Q^2 multi-shift CGM, 32^3x64, 8 masses log-spaced in [0.002, 0.2], 3 Z2 sources",
+                    T=64, L=32, eps=0.35, seed=1, kappa=0.1632, masses=list(np.geomspace(0.002, 0.2, 8)),
+                    residue=1e-20, bc_t=-1.0)
+
+
+def run_cgm(args):
+    """The multi-shift workload (one step = one source solved for all 8 masses,
+    FP32 multi-shift + per-shift mixed refinement, every shift to |r|/|b| <=
+    1e-10 checked in FP64); reported as an extra line, not the headline."""
+    import torch
+    from nissa_b200 import Lattice
+    from nissa_b200 import workload as wl
+    W = dict(CGM_WORKLOAD)
+    if args.lattice:
+        W["T"], W["L"] = (int(x) for x in args.lattice.split(","))
+    T, L = W["T"], W["L"]
+    V = T * L ** 3
+    conf = wl.gauge_conf(T, L, W["eps"], W["seed"], device="cuda:0")
+    lat = Lattice(T, L, bc_t=W["bc_t"])
+    lat.upload_conf(conf)
+    srcs = [torch.from_numpy(wl.z2_source(T, L, 100 + c, col=c)).cuda() for c in range(3)]
+    outs = [torch.empty((V, 4, 3, 2), dtype=torch.float64, device="cuda") for _ in W["masses"]]
+    res = {}
+    for prec in (args.cgm_precision, "double"):
+        lat.inv_tmQ2_cgm(W["kappa"], W["masses"], srcs[0], 100000, W["residue"], precision=prec, out=outs)  # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        stats = []
+        for c in range(3):
+            _, st = lat.inv_tmQ2_cgm(W["kappa"], W["masses"], srcs[c], 100000, W["residue"], precision=prec,
+                                     out=outs)
+            stats.append(st)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res[prec] = {"sources_per_s": 3 / dt, "s_per_source": dt / 3,
+                     "iterations": [s["iterations"] for s in stats[0]],
+                     "true_rel_res2_max": max(x["true_rel_res2"] for st in stats for x in st)}
+    print(json.dumps({"workload": W["name"].replace("32^3x64", "%d^3x%d" % (L, T)), "kappa": W["kappa"],
+                      "masses": W["masses"], "residue_sq": W["residue"], "mixed": res[args.cgm_precision],
+                      "fp64": res["double"],
+                      "mixed_speedup_vs_fp64": res["double"]["s_per_source"] / res[args.cgm_precision]["s_per_source"]}),
+          flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -348,12 +392,18 @@ def main():
                     help="only time the e/o hopping kernel of this precision (profiling entry point)")
     ap.add_argument("--variant", type=int, default=1, help="hopping kernel variant for --kernel-only")
     ap.add_argument("--nrep", type=int, default=10, help="launches for --kernel-only")
+    ap.add_argument("--workload", default="cg", choices=["cg", "cgm"],
+                    help="cg: the headline solve; cgm: the multi-shift workload (extra report)")
+    ap.add_argument("--cgm-precision", default="single", choices=["single", "half"])
     args = ap.parse_args()
     if args.lattice:
         T, L = (int(x) for x in args.lattice.split(","))
         WORKLOAD.update(T=T, L=L, name=WORKLOAD["name"].replace("32^3x64", "%d^3x%d" % (L, T)))
     if args.kernel_only:
         run_kernel_only(args)
+        return
+    if args.workload == "cgm":
+        run_cgm(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)

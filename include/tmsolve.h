@@ -131,6 +131,24 @@ tms_status tms_cg_eoprec_square(tms_ctx *ctx, double *sol, const double *guess, 
 tms_status tms_cg_eoprec(tms_ctx *ctx, double *sol_lx, const double *src_lx, double kappa, int has_anis,
                          double anis, double mu, int niter, double residue, int precision, tms_stats *stats);
 
+/* inv_tmQ2_cg: inverters/twisted_mass/cg_invert_tmQ2_common.cpp:5 (a CRASH("reimplement") stub in the
+ * reference, cg_invert_tmQ2.cpp:12-14).  Full-lattice CG on Q(+m)Q(-m) = Q_W^2 + m^2 (lx spinors);
+ * guess may be NULL. */
+tms_status tms_cg_tmQ2(tms_ctx *ctx, double *sol_lx, const double *guess_lx, const double *src_lx, double kappa,
+                       int has_anis, double anis, double m, int niter, double residue, int precision,
+                       tms_stats *stats);
+/* inv_tmQ2_cgm: inverters/twisted_mass/cgm_invert_tmQ2.cpp:46-53 (stub behind it) and its working
+ * counterpart inv_tmclovQ2_cgm at zero clover (inverters/twisted_clover/cgm_invert_tmclovQ2.cpp:10-32,
+ * cgm_invert in inverters/templates/cgm_invert_template_threaded.hpp:11-295).
+ * Solves (Q_W^2 + m_k^2) sol_k = src for nmass (<= 32) masses at once; sols is an array of nmass lx
+ * spinors (nissa's spincolor**), residues the per-shift squared relative residues.  TMS_PREC_DOUBLE is
+ * the reference's FP64 multi-shift CG; the mixed precisions run it in FP32 down to |r|/|b| = 1e-6 and
+ * bring each shift to its target with the mixed-precision CG of tms_cg_tmQ2 from that guess, checking
+ * every shift's true residual in FP64.  stats (may be NULL) receives nmass entries. */
+tms_status tms_cgm_tmQ2(tms_ctx *ctx, double *const *sols, const double *src_lx, double kappa, int has_anis,
+                        double anis, const double *masses, int nmass, int niter, const double *residues,
+                        int precision, tms_stats *stats);
+
 /* ---- instrumentation (no reference counterpart) ---- */
 
 /* Number of CUDA kernels this context has launched (CUDA-graph replays count their nodes). */

@@ -1,0 +1,667 @@
+// C ABI of the solvers: the e/o CG of K(+mu)K(-mu) (FP64, and FP32 / FP16
+// inner with FP64 reliable updates), the full solve of Eq. (8)-(11), the
+// full-lattice CG of Q(+m)Q(-m) and the multi-shift CGM of the tm Q^2
+// operator.  Each CG/CGM iteration block is replayed as a CUDA graph.
+#include "tms_internal.cuh"
+
+#include <algorithm>
+
+using namespace tms_int;
+
+namespace
+{
+  // ================================================================ operators
+  // A CG "operator policy" fixes the matrix, the fields it works on and the
+  // number of sites of its vectors.
+  //   EoOp: K(+mu)K(-mu) on odd sites (inv_tmDkern_eoprec_square_eos_cg)
+  //   LxOp: Q(+mu)Q(-mu) on the full lattice (inv_tmQ2_cg, and the per-shift
+  //         refinement of the multi-shift solver)
+  // hi fields (FP64): 0 b, 1 x, 2 r, 3 p, 4-6 temporaries; lo fields (inner
+  // precision): 1 r, 2 p, 3-4 temporaries.
+
+  struct EoOp
+  {
+    static constexpr int slot0 = 0;
+    static constexpr int nlo = 6;
+    static int stride(tms_ctx* c) { return c->g.stride; }
+    static int nsites(tms_ctx* c) { return (int)c->g.Vh; }
+    static Field* hi(tms_ctx* c) { return c->f64; }
+    static Field* lo(tms_ctx* c) { return c->lo; }
+    static int& lo_prec(tms_ctx* c) { return c->lo_prec; }
+    static Field& xlo(tms_ctx* c) { return c->xlo32; }
+
+    // r = b - K(+mu)K(-mu) x in FP64; returns |r|^2 (uses hi 4, 5, 6)
+    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr)
+    {
+      Field &t1 = ctx->f64[4], &te = ctx->f64[5], &s = ctx->f64[6];
+      auto U = links64(ctx);
+      kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
+      kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
+      const int n = nsites(ctx);
+      ++ctx->launches;
+      residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+        n, view<PREC_F64>(b), view<PREC_F64>(s), view<PREC_F64>(r), reducer(ctx));
+      CU(cudaGetLastError());
+      *rr = read_result(ctx);
+      return TMS_OK;
+    }
+
+    // `iters` CG iterations in precision P (x in PX): v 1 r, 2 p, 3 t1, 4 te
+    template <int P, int PX, int LF>
+    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters)
+    {
+      const Field &r = v[1], &p = v[2], &t1 = v[3], &te = v[4];
+      const int* stop = &c->st->stop;
+      const OpParams* prm = c->prm;
+      for (int it = 0; it < iters; it++)
+        {
+          EpiInvDiag<P> a1{{view<P>(te), view<P>(te)}, prm, -1.0};
+          launch_hop<P, LF>(c, s, 0, 1, p, p, U, prm, a1, NoFin{}, stop);
+          EpiKern<P, true> b1{{view<P>(t1), view<P>(t1)}, {view<P>(p), view<P>(p)}, prm, -1.0};
+          launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b1, FinAlpha{c->st}, stop);
+          EpiInvDiag<P> a2{{view<P>(te), view<P>(te)}, prm, +1.0};
+          launch_hop<P, LF>(c, s, 0, 1, t1, t1, U, prm, a2, NoFin{}, stop);
+          EpiKernCgUpdate<P, PX> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), prm, c->st, +1.0};
+          launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+          const int n = nsites(c);
+          ++c->launches;
+          xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s>>>(n, view<P>(r), view<P>(p), c->st, stop);
+        }
+    }
+  };
+
+  struct LxOp
+  {
+    static constexpr int slot0 = 3;
+    static constexpr int nlo = 5;
+    static int stride(tms_ctx* c) { return 2 * c->g.stride; }
+    static int nsites(tms_ctx* c) { return 2 * c->g.stride; }
+    static Field* hi(tms_ctx* c) { return c->lx64; }
+    static Field* lo(tms_ctx* c) { return c->lxlo; }
+    static int& lo_prec(tms_ctx* c) { return c->lxlo_prec; }
+    static Field& xlo(tms_ctx* c) { return c->lxxlo; }
+
+    template <int P>
+    static void qop(tms_ctx* c, cudaStream_t s, const Field& in, const Field& out, double sgn, const OpParams* prm)
+    {
+      EpiTmQ<P, false> e{{view_par<P>(out, 0), view_par<P>(out, 1)}, {view_par<P>(in, 0), view_par<P>(in, 1)}, prm,
+                         sgn};
+      launch_hop_v<P, LINK_F64_18>(c, s, 0, 2, view_par<P>(in, 0), view_par<P>(in, 1), links64(c), prm, e);
+    }
+
+    // r = b - Q(+mu)Q(-mu) x in FP64; returns |r|^2 (uses hi 4, 5)
+    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr)
+    {
+      Field &t = ctx->lx64[4], &s = ctx->lx64[5];
+      qop<PREC_F64>(ctx, ctx->stream, x, t, -1.0, ctx->prm);
+      qop<PREC_F64>(ctx, ctx->stream, t, s, +1.0, ctx->prm);
+      const int n = nsites(ctx);
+      ++ctx->launches;
+      residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+        n, view<PREC_F64>(b), view<PREC_F64>(s), view<PREC_F64>(r), reducer(ctx));
+      CU(cudaGetLastError());
+      *rr = read_result(ctx);
+      return TMS_OK;
+    }
+
+    // `iters` CG iterations: t = Q(-mu) p reducing |t|^2 ; s = Q(+mu) t fused
+    // with the x and r updates ; p = r + beta p.   v 1 r, 2 p, 3 t
+    template <int P, int PX, int LF>
+    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters)
+    {
+      const Field &r = v[1], &p = v[2], &t = v[3];
+      const int* stop = &c->st->stop;
+      const OpParams* prm = c->prm;
+      auto V = [](const Field& f, int par) { return view_par<P>(f, par); };
+      for (int it = 0; it < iters; it++)
+        {
+          EpiTmQ<P, true> a{{V(t, 0), V(t, 1)}, {V(p, 0), V(p, 1)}, prm, -1.0};
+          launch_hop_v<P, LF>(c, s, 0, 2, V(p, 0), V(p, 1), U, prm, a, FinAlpha{c->st}, stop);
+          EpiTmQCgUpdate<P, PX> b{{V(t, 0), V(t, 1)},
+                                  {V(r, 0), V(r, 1)},
+                                  {V(p, 0), V(p, 1)},
+                                  {view_par<PX>(x, 0), view_par<PX>(x, 1)},
+                                  prm,
+                                  c->st,
+                                  +1.0};
+          launch_hop_v<P, LF>(c, s, 0, 2, V(t, 0), V(t, 1), U, prm, b, FinBeta{c->st}, stop);
+          const int n = nsites(c);
+          ++c->launches;
+          xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s>>>(n, view<P>(r), view<P>(p), c->st, stop);
+        }
+    }
+  };
+
+  // capture a block of iterations once per (slot, fields); replayed every launch
+  template <class Rec>
+  tms_status capture(tms_ctx* ctx, int slot, const Rec& rec)
+  {
+    if (ctx->graph[slot]) return TMS_OK;
+    cudaStream_t cs;
+    CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph;
+    CU(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = ctx->launches;
+    rec(cs);
+    ctx->graph_nodes[slot] = ctx->launches - before;
+    ctx->launches = before;
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ctx->graph[slot], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return TMS_OK;
+  }
+
+  tms_status drop_graph(tms_ctx* ctx, int slot)
+  {
+    if (ctx->graph[slot])
+      {
+        CU(cudaStreamSynchronize(ctx->stream));
+        cudaGraphExecDestroy(ctx->graph[slot]);
+        ctx->graph[slot] = nullptr;
+      }
+    return TMS_OK;
+  }
+
+  tms_status launch_graph(tms_ctx* ctx, int slot)
+  {
+    CU(cudaGraphLaunch(ctx->graph[slot], ctx->stream));
+    ctx->launches += ctx->graph_nodes[slot];
+    return TMS_OK;
+  }
+
+  void fill_stats(tms_stats* stats, tms_status st, int iters, int reliable, double it_res, double true_res, float ms)
+  {
+    if (!stats) return;
+    stats->status = st;
+    stats->iterations = iters;
+    stats->reliable_updates = reliable;
+    stats->iterated_rel_res2 = it_res;
+    stats->true_rel_res2 = true_res;
+    stats->seconds = ms * 1e-3;
+  }
+
+  // ------------------------------------------------------------- CG, FP64
+  // b = hi[0], x = hi[1] (initial guess / solution).  cg_invert
+  // (cg_invert_template_threaded.hpp:17-150) with the operator of the policy.
+  template <class Op>
+  tms_status cg_double(tms_ctx* ctx, int niter, double residue, bool have_guess, tms_stats* stats)
+  {
+    Field* f = Op::hi(ctx);
+    const int n = Op::nsites(ctx);
+    for (int i = 1; i <= 6; i++) TRY(alloc_field(ctx, f[i], PREC_F64, Op::stride(ctx)));
+    double b2;
+    TRY(norm2<PREC_F64>(ctx, f[0], &b2, n));
+    if (b2 == 0.0 || std::isnan(b2)) return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm: %g", b2);
+    double rr;
+    if (have_guess) TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rr));
+    else
+      {
+        CU(cudaMemsetAsync(f[1].d, 0, f[1].bytes, ctx->stream));
+        CU(cudaMemcpyAsync(f[2].d, f[0].d, f[0].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        rr = b2;
+      }
+    CU(cudaMemcpyAsync(f[3].d, f[2].d, f[2].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    CgState& S = *ctx->st_h;
+    memset(&S, 0, sizeof S);
+    S.rr = rr;
+    S.b2 = b2;
+    S.target = residue * b2;
+    S.rel_trigger = -1.0;
+    S.niter_max = niter;
+    S.stop = (rr < S.target) ? STOP_CONVERGED : STOP_RUN;
+    TRY(push_state(ctx));
+    auto U = links64(ctx);
+    Field v[5] = {Field{}, f[2], f[3], f[4], f[5]};
+    const int slot = Op::slot0;
+    TRY(capture(ctx, slot, [&](cudaStream_t cs) {
+      Op::template record<PREC_F64, PREC_F64>(ctx, cs, U, v, f[1], ctx->graph_iters);
+    }));
+    CU(cudaEventRecord(ctx->ev0, ctx->stream));
+    while (S.stop == STOP_RUN)
+      {
+        TRY(launch_graph(ctx, slot));
+        TRY(pull_state(ctx));
+      }
+    CU(cudaEventRecord(ctx->ev1, ctx->stream));
+    double tr;
+    TRY(Op::true_residual(ctx, f[0], f[1], f[6], &tr));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    tms_status st = TMS_OK;
+    if (S.stop == STOP_BREAKDOWN) st = fail(ctx, TMS_ERR_NAN, "nanned (iteration %d)", S.iter);
+    else if (S.stop == STOP_MAXITER) st = fail(ctx, TMS_ERR_NOT_CONVERGED, "exit without converging");
+    fill_stats(stats, st, S.iter, 0, S.rr / b2, tr / b2, ms);
+    return st;
+  }
+
+  // ------------------------------------------------- CG, mixed precision
+  // FP32 (or FP16-spinor) inner CG with FP64 reliable updates: the solution is
+  // accumulated in FP64 and the residual recomputed with the FP64 operator
+  // whenever the iterated residual has dropped by delta since the last update
+  // (the outer defect-correction loop of cg_128_invert_template_threaded.cpp:36-109,
+  // here with the Krylov direction kept across updates).
+  template <class Op, int P, int LF>
+  tms_status cg_mixed(tms_ctx* ctx, const LinkT<LF>& U, int niter, double residue, bool have_guess,
+                      tms_stats* stats)
+  {
+    constexpr int PX = (P == PREC_F16) ? PREC_F32 : P; // x accumulates in FP32 at least
+    const int slot = Op::slot0 + (P == PREC_F16 ? 2 : 1);
+    const int n = Op::nsites(ctx);
+    Field* f = Op::hi(ctx);
+    for (int i = 1; i <= 6; i++) TRY(alloc_field(ctx, f[i], PREC_F64, Op::stride(ctx)));
+    Field* lo = Op::lo(ctx);
+    if (Op::lo_prec(ctx) != P)
+      {
+        // the inner-precision fields move: graphs captured on the old ones are void
+        // (the FP32 multi-shift graph uses the full-lattice inner fields too)
+        TRY(drop_graph(ctx, Op::slot0 + 1));
+        TRY(drop_graph(ctx, Op::slot0 + 2));
+        if (Op::slot0 == LxOp::slot0) TRY(drop_graph(ctx, 7));
+        for (int i = 0; i < Op::nlo; i++) TRY(alloc_field(ctx, lo[i], P, Op::stride(ctx)));
+        Op::lo_prec(ctx) = P;
+      }
+    Field& xlo = Op::xlo(ctx);
+    TRY(alloc_field(ctx, xlo, PX, Op::stride(ctx)));
+    const double delta = (P == PREC_F16) ? 0.1 : 0.05; // reliable-update trigger (residual reduction)
+    double b2;
+    TRY(norm2<PREC_F64>(ctx, f[0], &b2, n));
+    if (b2 == 0.0 || std::isnan(b2)) return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm: %g", b2);
+    double rr;
+    if (have_guess) TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rr));
+    else
+      {
+        CU(cudaMemsetAsync(f[1].d, 0, f[1].bytes, ctx->stream));
+        CU(cudaMemcpyAsync(f[2].d, f[0].d, f[0].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        rr = b2;
+      }
+    const double target = residue * b2;
+    CgState& S = *ctx->st_h;
+    memset(&S, 0, sizeof S);
+    int reliable = 0;
+    float ms = 0;
+    tms_status st = TMS_OK;
+    if (rr >= target)
+      {
+        convert<P, PREC_F64>(ctx, f[2], lo[1], 1.0, n); // r_lo = r
+        convert<P, PREC_F64>(ctx, f[2], lo[2], 1.0, n); // p_lo = r
+        CU(cudaMemsetAsync(xlo.d, 0, xlo.bytes, ctx->stream));
+        S.rr = rr;
+        S.b2 = b2;
+        S.target = target;
+        S.rel_trigger = delta * delta * rr;
+        S.niter_max = niter;
+        S.stop = STOP_RUN;
+        TRY(push_state(ctx));
+        Field v[5] = {Field{}, lo[1], lo[2], lo[3], lo[4]};
+        TRY(capture(ctx, slot, [&](cudaStream_t cs) {
+          Op::template record<P, PX>(ctx, cs, U, v, xlo, ctx->graph_iters);
+        }));
+        CU(cudaEventRecord(ctx->ev0, ctx->stream));
+        for (;;)
+          {
+            TRY(launch_graph(ctx, slot));
+            TRY(pull_state(ctx));
+            if (S.stop == STOP_RUN) continue;
+            if (S.stop == STOP_BREAKDOWN)
+              {
+                st = fail(ctx, TMS_ERR_NAN, "nanned (iteration %d)", S.iter);
+                break;
+              }
+            // reliable update: x += x_lo (FP64), r = b - A x (FP64)
+            ++ctx->launches;
+            axpby_kernel<PREC_F64, PREC_F64, PX><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+              n, 1.0, view<PREC_F64>(f[1]), 1.0, view<PX>(xlo), view<PREC_F64>(f[1]));
+            CU(cudaMemsetAsync(xlo.d, 0, xlo.bytes, ctx->stream));
+            if (xlo.n) CU(cudaMemsetAsync(xlo.n, 0, sizeof(float) * xlo.stride, ctx->stream));
+            double rt;
+            TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rt));
+            reliable++;
+            if (rt < target) break;
+            if (S.stop == STOP_MAXITER || S.iter >= niter)
+              {
+                st = fail(ctx, TMS_ERR_NOT_CONVERGED, "exit without converging");
+                break;
+              }
+            // restart the recurrence from the true residual, keeping the direction
+            convert<P, PREC_F64>(ctx, f[2], lo[1], 1.0, n);
+            S.beta = rt / S.rr_prev;
+            S.rr = rt;
+            S.rel_trigger = delta * delta * rt;
+            S.stop = STOP_RUN;
+            TRY(push_state(ctx));
+            ++ctx->launches;
+            xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, view<P>(lo[1]),
+                                                                                       view<P>(lo[2]), ctx->st,
+                                                                                       nullptr);
+            CU(cudaGetLastError());
+          }
+        CU(cudaEventRecord(ctx->ev1, ctx->stream));
+        CU(cudaEventSynchronize(ctx->ev1));
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+      }
+    double tr;
+    TRY(Op::true_residual(ctx, f[0], f[1], f[6], &tr));
+    fill_stats(stats, st, S.iter, reliable, S.rr / b2, tr / b2, ms);
+    return st;
+  }
+
+  template <class Op>
+  tms_status cg_dispatch(tms_ctx* ctx, int precision, int niter, double residue, bool have_guess, tms_stats* stats)
+  {
+    if (precision == TMS_PREC_DOUBLE) return cg_double<Op>(ctx, niter, residue, have_guess, stats);
+    if (precision == TMS_PREC_MIXED_SINGLE)
+      return ctx->su3 ? cg_mixed<Op, PREC_F32>(ctx, links32r(ctx), niter, residue, have_guess, stats)
+                      : cg_mixed<Op, PREC_F32>(ctx, links32f(ctx), niter, residue, have_guess, stats);
+    if (precision == TMS_PREC_MIXED_HALF)
+      return ctx->su3 ? cg_mixed<Op, PREC_F16>(ctx, links32r(ctx), niter, residue, have_guess, stats)
+                      : cg_mixed<Op, PREC_F16>(ctx, links32f(ctx), niter, residue, have_guess, stats);
+    return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
+  }
+
+  // ------------------------------------------------------ multi-shift CGM
+  // cgm_invert (cgm_invert_template_threaded.hpp:11-295) on Q_W^2 = Q(0)Q(0),
+  // shifts sigma_i = m_i^2, for the source in lx64[0].  Vectors in precision P;
+  // solutions left in ctx->cgm_x.  Returns the solver status, *iters the
+  // iteration count (the reference's final_iter).
+  size_t per_site_bytes(int prec) { return prec == PREC_F64 ? 192 : prec == PREC_F32 ? 96 : 52; }
+
+  template <int P, int LF>
+  tms_status cgm_run(tms_ctx* ctx, const LinkT<LF>& U, int nshift, const double* sigma, const double* target,
+                     int niter, double b2, int* iters, float* ms)
+  {
+    const int slot = (P == PREC_F64) ? 6 : 7;
+    const int stride = 2 * ctx->g.stride, n = stride;
+    const size_t fbytes = per_site_bytes(P) * (size_t)stride;
+    if (ctx->cgm_prec != P || ctx->cgm_nshift < nshift)
+      {
+        TRY(drop_graph(ctx, 6));
+        TRY(drop_graph(ctx, 7));
+        if (ctx->cgm_x) cudaFree(ctx->cgm_x);
+        if (ctx->cgm_ps) cudaFree(ctx->cgm_ps);
+        ctx->cgm_x = ctx->cgm_ps = nullptr;
+        ctx->cgm_prec = -1;
+        CU(cudaMalloc(&ctx->cgm_x, fbytes * nshift));
+        CU(cudaMalloc(&ctx->cgm_ps, fbytes * nshift));
+        ctx->cgm_prec = P;
+        ctx->cgm_nshift = nshift;
+      }
+    // inner vectors: r, p, t in precision P (FP64: hi 2-4, otherwise lo 1-3)
+    if (P == PREC_F64)
+      {
+        for (int i = 2; i <= 4; i++) TRY(alloc_field(ctx, ctx->lx64[i], PREC_F64, stride));
+      }
+    else if (ctx->lxlo_prec != P)
+      {
+        TRY(drop_graph(ctx, LxOp::slot0 + 1));
+        TRY(drop_graph(ctx, LxOp::slot0 + 2));
+        for (int i = 0; i < LxOp::nlo; i++) TRY(alloc_field(ctx, ctx->lxlo[i], P, stride));
+        ctx->lxlo_prec = P;
+      }
+    const bool hi = (P == PREC_F64);
+    const Field& r = hi ? ctx->lx64[2] : ctx->lxlo[1];
+    const Field& p = hi ? ctx->lx64[3] : ctx->lxlo[2];
+    const Field& t = hi ? ctx->lx64[4] : ctx->lxlo[3];
+    // solution / direction views of shift k
+    auto shift_field = [&](void* base, int k) {
+      Field f;
+      f.prec = P;
+      f.d = (unsigned char*)base + fbytes * k;
+      f.n = nullptr;
+      f.stride = stride;
+      f.bytes = fbytes;
+      return f;
+    };
+    // r = p = b ; ps_i = b ; x_i = 0
+    convert<P, PREC_F64>(ctx, ctx->lx64[0], r, 1.0, n);
+    convert<P, PREC_F64>(ctx, ctx->lx64[0], p, 1.0, n);
+    for (int k = 0; k < nshift; k++) convert<P, PREC_F64>(ctx, ctx->lx64[0], shift_field(ctx->cgm_ps, k), 1.0, n);
+    CU(cudaMemsetAsync(ctx->cgm_x, 0, fbytes * nshift, ctx->stream));
+    CgmState& S = *ctx->cgm_h;
+    memset(&S, 0, sizeof S);
+    S.rr = b2;
+    S.b2 = b2;
+    S.betaa = 1.0;
+    S.alpha = 0.0;
+    S.nshift = nshift;
+    S.nrun = nshift;
+    S.niter_max = niter;
+    for (int k = 0; k < nshift; k++)
+      {
+        S.sigma[k] = sigma[k];
+        S.target[k] = target[k];
+        S.zps[k] = S.zas[k] = 1.0;
+        S.alphas[k] = 0.0;
+        S.run[k] = 1;
+      }
+    CU(cudaMemcpyAsync(ctx->cgm, &S, sizeof S, cudaMemcpyHostToDevice, ctx->stream));
+    const OpParams* prm = ctx->prm + 1; // the CGM operator: mu = 0
+    const size_t shift_elems = fbytes / (P == PREC_F64 ? sizeof(double2) : P == PREC_F32 ? sizeof(float4) : sizeof(uint4));
+    TRY(capture(ctx, slot, [&](cudaStream_t cs) {
+      auto V = [](const Field& f, int par) { return view_par<P>(f, par); };
+      const int* stop = &ctx->cgm->stop;
+      for (int it = 0; it < ctx->graph_iters; it++)
+        {
+          ++ctx->launches;
+          cgm_begin_kernel<<<1, 1, 0, cs>>>(ctx->cgm);
+          EpiTmQ<P, true> a{{V(t, 0), V(t, 1)}, {V(p, 0), V(p, 1)}, prm, +1.0};
+          launch_hop_v<P, LF>(ctx, cs, 0, 2, V(p, 0), V(p, 1), U, prm, a, FinCgm1{ctx->cgm}, stop);
+          EpiCgm2<P> b{{V(t, 0), V(t, 1)}, {V(r, 0), V(r, 1)}, prm, ctx->cgm};
+          launch_hop_v<P, LF>(ctx, cs, 0, 2, V(t, 0), V(t, 1), U, prm, b, FinCgm2{ctx->cgm}, stop);
+          ++ctx->launches;
+          cgm_update_kernel<P><<<div_up(n, 256), 256, 0, cs>>>(n, view<P>(r), view<P>(p),
+                                                               view<P>(shift_field(ctx->cgm_x, 0)),
+                                                               view<P>(shift_field(ctx->cgm_ps, 0)), shift_elems,
+                                                               ctx->cgm);
+        }
+    }));
+    CU(cudaEventRecord(ctx->ev0, ctx->stream));
+    do
+      {
+        TRY(launch_graph(ctx, slot));
+        CU(cudaMemcpyAsync(ctx->cgm_h, ctx->cgm, sizeof(CgmState), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+      }
+    while (S.stop == STOP_RUN);
+    CU(cudaEventRecord(ctx->ev1, ctx->stream));
+    CU(cudaEventSynchronize(ctx->ev1));
+    cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+    *iters = S.iter;
+    if (S.stop == STOP_BREAKDOWN) return fail(ctx, TMS_ERR_NAN, "nanned (cgm iteration %d)", S.iter);
+    if (S.stop == STOP_MAXITER) return fail(ctx, TMS_ERR_NOT_CONVERGED, "exit without converging");
+    return TMS_OK;
+  }
+
+  // x (FP64 full field) = solution of shift k of the last CGM
+  template <int P>
+  void cgm_solution(tms_ctx* ctx, int k, const Field& x)
+  {
+    const int stride = 2 * ctx->g.stride;
+    Field f;
+    f.prec = P;
+    f.d = (unsigned char*)ctx->cgm_x + per_site_bytes(P) * (size_t)stride * k;
+    f.stride = stride;
+    convert<PREC_F64, P>(ctx, f, x, 1.0, stride);
+  }
+}
+
+extern "C" {
+
+tms_status tms_cg_eoprec_square(tms_ctx* ctx, double* sol, const double* guess, const double* src, double kappa,
+                                int has_anis, double anis, double mu, int niter, double residue, int precision,
+                                tms_stats* stats)
+{
+  TRY(check_conf(ctx));
+  if (!sol || !src || niter <= 0 || !(residue > 0)) return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
+  TRY(set_params(ctx, kappa, mu, has_anis, anis));
+  Field* f = ctx->f64;
+  TRY(spinor_in(ctx, src, nullptr, ctx->g.Vh, f[0]));
+  if (guess) TRY(spinor_in(ctx, guess, nullptr, ctx->g.Vh, f[1]));
+  const tms_status st = cg_dispatch<EoOp>(ctx, precision, niter, residue, guess != nullptr, stats);
+  if (st == TMS_OK || st == TMS_ERR_NOT_CONVERGED) TRY(spinor_out(ctx, f[1], nullptr, ctx->g.Vh, sol, true));
+  TRY(finish(ctx));
+  return st;
+}
+
+tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, double kappa, int has_anis, double anis,
+                         double mu, int niter, double residue, int precision, tms_stats* stats)
+{
+  TRY(check_conf(ctx));
+  if (!sol_lx || !src_lx || niter <= 0 || !(residue > 0)) return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
+  TRY(set_params(ctx, kappa, mu, has_anis, anis));
+  Field* f = ctx->f64;
+  for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
+  Field *eta = ctx->ex, *psi = ctx->ex + 2; // [0] even, [1] odd
+  for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
+  const int64_t Vh = ctx->g.Vh;
+  const int n = (int)Vh;
+  const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
+  auto V = [&](const Field& x) { return view<PREC_F64>(x); };
+  auto U = links64(ctx);
+  // split_lx_vector_into_eo_parts(source)
+  const double* src = src_lx;
+  if (ctx->ptr_mode == TMS_PTR_HOST)
+    {
+      TRY(ensure_stage(ctx, bytes));
+      CU(cudaMemcpyAsync(ctx->stage, src_lx, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      src = ctx->stage;
+    }
+  ++ctx->launches;
+  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(eta[0]));
+  ++ctx->launches;
+  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
+  // Eq. (8a): te = D_ee^-1 eta_e ; Eq. (8b): varphi = g5 (eta_o + hop(te)/2) -> f0
+  ++ctx->launches;
+  diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(eta[0]), V(f[5]), ctx->prm, 1.0, 1);
+  EpiSrcPrep<PREC_F64> sp{{V(f[0]), V(f[0])}, {V(eta[1]), V(eta[1])}};
+  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
+  CU(cudaGetLastError());
+  // Eq. (9)
+  const tms_status st = cg_dispatch<EoOp>(ctx, precision, niter, residue, false, stats);
+  if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+  // Eq. (10): psi_o = K(-mu) x ; Eq. (11): psi_e = D_ee^-1 (eta_e + hop(psi_o)/2)
+  kern_op<PREC_F64>(ctx, U, f[1], f[5], psi[1], -1.0, ctx->prm);
+  EpiReco<PREC_F64> rc{{V(psi[0]), V(psi[0])}, {V(eta[0]), V(eta[0])}, ctx->prm, 1.0};
+  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
+  CU(cudaGetLastError());
+  // paste_eo_parts_into_lx_vector
+  double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sol_lx;
+  ++ctx->launches;
+  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, d);
+  ++ctx->launches;
+  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, d);
+  CU(cudaGetLastError());
+  if (ctx->ptr_mode == TMS_PTR_HOST) CU(cudaMemcpyAsync(sol_lx, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  // lx residual check (cg_invert_tmD_eoprec.cpp:192-212): |g5 Q sol - src|^2 / |src|^2
+  if (stats)
+    {
+      EpiTmQ<PREC_F64, false> e{{V(f[2]), V(f[3])}, {V(psi[0]), V(psi[1])}, ctx->prm, +1.0};
+      launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 2, psi[0], psi[1], U, ctx->prm, e);
+      double num = 0, den = 0;
+      for (int par = 0; par < 2; par++)
+        {
+          ++ctx->launches;
+          g5_residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, V(f[2 + par]), V(eta[par]),
+                                                                                       reducer(ctx));
+          CU(cudaGetLastError());
+          num += read_result(ctx);
+          double e2;
+          TRY(norm2<PREC_F64>(ctx, eta[par], &e2));
+          den += e2;
+        }
+      stats->lx_rel_res2 = num / den;
+    }
+  TRY(finish(ctx));
+  return st;
+}
+
+
+tms_status tms_cg_tmQ2(tms_ctx* ctx, double* sol_lx, const double* guess_lx, const double* src_lx, double kappa,
+                       int has_anis, double anis, double m, int niter, double residue, int precision,
+                       tms_stats* stats)
+{
+  TRY(check_conf(ctx));
+  if (!sol_lx || !src_lx || niter <= 0 || !(residue > 0)) return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
+  TRY(set_params(ctx, kappa, m, has_anis, anis));
+  Field* f = ctx->lx64;
+  TRY(lx_in(ctx, src_lx, f[0]));
+  if (guess_lx) TRY(lx_in(ctx, guess_lx, f[1]));
+  const tms_status st = cg_dispatch<LxOp>(ctx, precision, niter, residue, guess_lx != nullptr, stats);
+  if (st == TMS_OK || st == TMS_ERR_NOT_CONVERGED) TRY(lx_out(ctx, f[1], sol_lx));
+  TRY(finish(ctx));
+  return st;
+}
+
+tms_status tms_cgm_tmQ2(tms_ctx* ctx, double* const* sols, const double* src_lx, double kappa, int has_anis,
+                        double anis, const double* masses, int nmass, int niter, const double* residues,
+                        int precision, tms_stats* stats)
+{
+  TRY(check_conf(ctx));
+  if (!sols || !src_lx || !masses || !residues || nmass <= 0 || nmass > CGM_MAX_SHIFTS || niter <= 0)
+    return fail(ctx, TMS_ERR_BAD_ARG, "bad multi-shift arguments (1 <= nmass <= %d)", CGM_MAX_SHIFTS);
+  if (precision != TMS_PREC_DOUBLE && precision != TMS_PREC_MIXED_SINGLE && precision != TMS_PREC_MIXED_HALF)
+    return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
+  for (int k = 0; k < nmass; k++)
+    if (!sols[k] || !(residues[k] > 0) || !std::isfinite(masses[k]))
+      return fail(ctx, TMS_ERR_BAD_ARG, "bad shift %d", k);
+  TRY(set_params(ctx, kappa, 0.0, has_anis, anis, 1)); // the CGM operator Q(0)^2
+  Field* f = ctx->lx64;
+  const int stride = 2 * ctx->g.stride;
+  for (int i = 1; i <= 6; i++) TRY(alloc_field(ctx, f[i], PREC_F64, stride));
+  TRY(lx_in(ctx, src_lx, f[0]));
+  double b2;
+  TRY(norm2<PREC_F64>(ctx, f[0], &b2, stride));
+  if (b2 == 0.0 || std::isnan(b2)) return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm: %g", b2);
+  double sigma[CGM_MAX_SHIFTS], target[CGM_MAX_SHIFTS];
+  // the FP32 multi-shift solve stops at |r|/|b| = 1e-6 at most; each shift is
+  // then brought to its target by the mixed-precision CG from that guess
+  const double floor32 = 1e-12;
+  for (int k = 0; k < nmass; k++)
+    {
+      sigma[k] = masses[k] * masses[k];
+      target[k] = (precision == TMS_PREC_DOUBLE) ? residues[k] : std::max(residues[k], floor32);
+    }
+  int iters = 0;
+  float ms = 0;
+  tms_status st;
+  if (precision == TMS_PREC_DOUBLE)
+    st = cgm_run<PREC_F64>(ctx, links64(ctx), nmass, sigma, target, niter, b2, &iters, &ms);
+  else
+    st = ctx->su3 ? cgm_run<PREC_F32>(ctx, links32r(ctx), nmass, sigma, target, niter, b2, &iters, &ms)
+                  : cgm_run<PREC_F32>(ctx, links32f(ctx), nmass, sigma, target, niter, b2, &iters, &ms);
+  if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+  tms_status worst = st;
+  for (int k = 0; k < nmass; k++)
+    {
+      if (precision == TMS_PREC_DOUBLE) cgm_solution<PREC_F64>(ctx, k, f[1]);
+      else cgm_solution<PREC_F32>(ctx, k, f[1]);
+      // final true residue of the shift (cgm_invert_template_threaded.hpp:266-279)
+      TRY(set_params(ctx, kappa, masses[k], has_anis, anis));
+      double rt;
+      TRY(LxOp::true_residual(ctx, f[0], f[1], f[2], &rt));
+      tms_stats sk{};
+      fill_stats(&sk, st, iters, 0, ctx->cgm_h->res[k], rt / b2, ms);
+      if (precision != TMS_PREC_DOUBLE && rt >= residues[k] * b2)
+        {
+          tms_stats rs{};
+          const tms_status s2 = cg_dispatch<LxOp>(ctx, precision, niter, residues[k], true, &rs);
+          if (s2 != TMS_OK && s2 != TMS_ERR_NOT_CONVERGED) return s2;
+          if (s2 != TMS_OK) worst = s2;
+          sk.iterations += rs.iterations;
+          sk.reliable_updates = rs.reliable_updates;
+          sk.iterated_rel_res2 = rs.iterated_rel_res2;
+          sk.true_rel_res2 = rs.true_rel_res2;
+          sk.seconds += rs.seconds;
+          sk.status = s2;
+        }
+      if (stats) stats[k] = sk;
+      TRY(lx_out(ctx, f[1], sols[k]));
+    }
+  TRY(finish(ctx));
+  if (worst != TMS_OK) return fail(ctx, worst, "exit without converging");
+  return TMS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,523 @@
+// Internal state and helpers of the C ABI shared by its translation units:
+// the context (tms_ctx), device fields, error handling, parameter upload,
+// kernel launch helpers and the boundary (AoS <-> SoA) transfers.
+#pragma once
+#include "tmsolve.h"
+#include "tms_kernels.cuh"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace tms;
+
+namespace tms_int
+{
+  inline int div_up(int64_t a, int b) { return (int)((a + b - 1) / b); }
+  inline int round_up(int64_t a, int b) { return (int)(((a + b - 1) / b) * b); }
+
+  // device spinor buffer of one precision, e/o sized (stride >= Vh)
+  struct Field
+  {
+    int prec = -1;
+    void* d = nullptr;
+    float* n = nullptr;
+    int stride = 0;
+    size_t bytes = 0;
+  };
+
+  template <int P>
+  SpinorT<P> view(const Field& f)
+  {
+    SpinorT<P> s;
+    s.d = reinterpret_cast<decltype(s.d)>(f.d);
+    s.n = f.n;
+    s.stride = f.stride;
+    return s;
+  }
+}
+
+using tms_int::Field;
+
+struct tms_ctx
+{
+  Lattice g{};
+  int device = 0;
+  int ptr_mode = TMS_PTR_HOST;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // geometry
+  int* lx_of_eo = nullptr; // [2][Vh] device
+
+  // gauge configuration
+  bool conf_loaded = false, su3 = false;
+  double2* U64 = nullptr;
+  float4* U32r = nullptr; // 12-real
+  float2* U32f = nullptr; // 18-real
+
+  // scalars and reduction scratch
+  OpParams* prm = nullptr;       // [2]: operator params (slot 0 solver, slot 1 free use)
+  CgState* st = nullptr;         // device solver state
+  CgState* st_h = nullptr;       // pinned host mirror
+  double* red_partial = nullptr;
+  unsigned* red_counter = nullptr;
+  double* red_result = nullptr;
+  double* red_h = nullptr;       // pinned
+  int red_cap = 0;
+
+  // staging for AoS conversions (device AoS doubles), grows on demand
+  double* stage = nullptr;
+  size_t stage_bytes = 0;
+
+  // work fields (allocated on first use)
+  Field f64[8];   // 0:b 1:x 2:r 3:p 4:t1 5:te(even) 6:s 7:tmp
+  Field lo[6];    // inner precision: 0:x 1:r 2:p 3:t1 4:te 5:spare
+  int lo_prec = -1;
+  Field xlo32;    // FP32 accumulator of x for the half-precision inner solver
+  Field ex[4];    // full solves: eta_e, eta_o, psi_e, psi_o
+
+  // full-lattice fields (both parities, plane stride 2*g.stride, parity p at offset p*g.stride)
+  Field lx64[8];  // 0:b 1:x 2:r 3:p 4:t 5:s 6,7:tmp
+  Field lxlo[5];  // inner precision: 1:r 2:p 3:t
+  int lxlo_prec = -1;
+  Field lxxlo;    // FP32 accumulator of x (full lattice)
+
+  // multi-shift CGM: state and the per-shift solutions / directions
+  CgmState* cgm = nullptr;
+  CgmState* cgm_h = nullptr;
+  void* cgm_x = nullptr;
+  void* cgm_ps = nullptr;
+  int cgm_prec = -1, cgm_nshift = 0;
+
+  // CUDA graphs of one iteration block: 0-2 e/o CG (FP64, FP32, FP16),
+  // 3-5 full-lattice CG (FP64, FP32, FP16), 6-7 CGM (FP64, FP32)
+  static constexpr int kGraphs = 8;
+  cudaGraphExec_t graph[kGraphs] = {};
+  int graph_iters = 8;
+  uint64_t graph_nodes[kGraphs] = {};
+
+  // kernels launched by this context (graph replays count their nodes)
+  uint64_t launches = 0;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace tms_int
+{
+  inline tms_status fail(tms_ctx* c, tms_status s, const char* fmt, ...)
+  {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return s;
+  }
+
+#define CU(call)                                                                                                 \
+  do                                                                                                             \
+    {                                                                                                            \
+      cudaError_t e_ = (call);                                                                                   \
+      if (e_ != cudaSuccess)                                                                                     \
+        return fail(ctx, e_ == cudaErrorMemoryAllocation ? TMS_ERR_OOM : TMS_ERR_CUDA, "%s: %s (%s:%d)", #call,  \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);                                                 \
+    }                                                                                                            \
+  while (0)
+
+#define TRY(...)                                                                                                 \
+  do                                                                                                             \
+    {                                                                                                            \
+      tms_status s_ = (__VA_ARGS__);                                                                             \
+      if (s_ != TMS_OK) return s_;                                                                               \
+    }                                                                                                            \
+  while (0)
+
+  inline tms_status alloc_field(tms_ctx* ctx, Field& f, int prec, int stride = 0)
+  {
+    if (stride == 0) stride = ctx->g.stride;
+    if (f.d && f.prec == prec && f.stride == stride) return TMS_OK;
+    if (f.d)
+      {
+        cudaFree(f.d);
+        f.d = nullptr;
+        if (f.n) cudaFree(f.n);
+        f.n = nullptr;
+      }
+    f.prec = prec;
+    f.stride = stride;
+    const size_t per = (prec == PREC_F64) ? 192 : (prec == PREC_F32) ? 96 : 48;
+    f.bytes = per * (size_t)f.stride;
+    CU(cudaMalloc(&f.d, f.bytes));
+    CU(cudaMemsetAsync(f.d, 0, f.bytes, ctx->stream));
+    if (prec == PREC_F16)
+      {
+        CU(cudaMalloc(&f.n, sizeof(float) * (size_t)f.stride));
+        CU(cudaMemsetAsync(f.n, 0, sizeof(float) * (size_t)f.stride, ctx->stream));
+      }
+    return TMS_OK;
+  }
+
+  inline tms_status ensure_stage(tms_ctx* ctx, size_t bytes)
+  {
+    if (ctx->stage_bytes >= bytes) return TMS_OK;
+    if (ctx->stage) cudaFree(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    CU(cudaMalloc(&ctx->stage, bytes));
+    ctx->stage_bytes = bytes;
+    return TMS_OK;
+  }
+
+  inline Reducer reducer(tms_ctx* c) { return Reducer{c->red_partial, c->red_counter, c->red_result}; }
+
+  inline tms_status set_params(tms_ctx* ctx, double kappa, double mu, int has_anis, double anis, int slot = 0)
+  {
+    if (!(kappa > 0.0) || !std::isfinite(kappa) || !std::isfinite(mu))
+      return fail(ctx, TMS_ERR_BAD_ARG, "invalid kappa %g / mu %g", kappa, mu);
+    OpParams h{kappa, mu, has_anis ? anis : 1.0};
+    CU(cudaMemcpyAsync(ctx->prm + slot, &h, sizeof h, cudaMemcpyHostToDevice, ctx->stream));
+    return TMS_OK;
+  }
+
+  // ------------------------------------------------------------ hop launch
+  template <int P, int LF, class Epi, class Fin = NoFin>
+  void launch_hop(tms_ctx* c, cudaStream_t s, int par_out, int npar, const Field& in_e, const Field& in_o,
+                  const LinkT<LF>& U, const OpParams* prm, const Epi& epi, const Fin& fin = Fin{},
+                  const int* stop = nullptr)
+  {
+    const int nsite = (int)(npar * c->g.Vh);
+    ++c->launches;
+    hop_kernel<P, LF, Epi, Fin><<<div_up(nsite, HOP_THREADS), HOP_THREADS, 0, s>>>(
+      c->g, par_out, npar, view<P>(in_e), view<P>(in_o), U, prm, epi, reducer(c), fin, stop);
+  }
+
+  inline LinkT<LINK_F64_18> links64(tms_ctx* c) { return LinkT<LINK_F64_18>{c->U64, (int)c->g.Vh}; }
+  inline LinkT<LINK_F32_12> links32r(tms_ctx* c) { return LinkT<LINK_F32_12>{c->U32r, (int)c->g.Vh}; }
+  inline LinkT<LINK_F32_18> links32f(tms_ctx* c) { return LinkT<LINK_F32_18>{c->U32f, (int)c->g.Vh}; }
+
+  // --------------------------------------------------------- conf kernels
+  static __global__ void conf_to_soa_kernel(Lattice g, const double* __restrict__ src, int layout, int unfold,
+                                     const int* __restrict__ lx_of_eo, double2* __restrict__ U)
+  {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= g.V) return;
+    const int p = idx >= g.Vh, ieo = idx - (p ? (int)g.Vh : 0);
+    const int lx = lx_of_eo[idx];
+    const size_t row = (layout == TMS_LAYOUT_LX) ? (size_t)lx : (size_t)idx;
+    const int t = lx / (g.LX * g.LY * g.LZ);
+    const double2* a = reinterpret_cast<const double2*>(src + row * 72);
+    for (int mu = 0; mu < 4; mu++)
+      {
+        const double sg = (unfold && mu == 0 && t == g.T - 1) ? g.bc_t : 1.0;
+        for (int k = 0; k < 9; k++)
+          {
+            const double2 w = a[mu * 9 + k];
+            U[((size_t)(p * 4 + mu) * 9 + k) * g.Vh + ieo] = make_double2(w.x * sg, w.y * sg);
+          }
+      }
+  }
+
+  // FP32 copies and the special-unitarity check (max deviation over links)
+  static __global__ void conf_lowprec_kernel(int64_t nlinks_per_parmu, int Vh, const double2* __restrict__ U,
+                                      float4* __restrict__ Ur, float2* __restrict__ Uf, Reducer red)
+  {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; // over 8*Vh (par,mu,site)
+    double dev = 0.0;
+    if (idx < nlinks_per_parmu)
+      {
+        const int pm = (int)(idx / Vh), site = (int)(idx - (int64_t)pm * Vh);
+        C<double> u[9];
+        for (int k = 0; k < 9; k++)
+          {
+            const double2 w = U[((size_t)pm * 9 + k) * Vh + site];
+            u[k] = {w.x, w.y};
+            Uf[((size_t)pm * 9 + k) * Vh + site] = make_float2((float)w.x, (float)w.y);
+          }
+        Ur[((size_t)pm * 3 + 0) * Vh + site] = make_float4((float)u[0].re, (float)u[0].im, (float)u[1].re, (float)u[1].im);
+        Ur[((size_t)pm * 3 + 1) * Vh + site] = make_float4((float)u[2].re, (float)u[2].im, (float)u[3].re, (float)u[3].im);
+        Ur[((size_t)pm * 3 + 2) * Vh + site] = make_float4((float)u[4].re, (float)u[4].im, (float)u[5].re, (float)u[5].im);
+        // deviation of row 2 from conj(row0 x row1), plus row-0/1 unitarity
+        const C<double> c0 = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
+        const C<double> c1 = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));
+        const C<double> c2 = cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));
+        dev = fmax(dev, fabs(c0.re - u[6].re) + fabs(c0.im - u[6].im));
+        dev = fmax(dev, fabs(c1.re - u[7].re) + fabs(c1.im - u[7].im));
+        dev = fmax(dev, fabs(c2.re - u[8].re) + fabs(c2.im - u[8].im));
+        double n0 = 0, n1 = 0;
+        C<double> d01 = {0, 0};
+        for (int k = 0; k < 3; k++)
+          {
+            n0 += u[k].re * u[k].re + u[k].im * u[k].im;
+            n1 += u[3 + k].re * u[3 + k].re + u[3 + k].im * u[3 + k].im;
+            d01 = cadd(d01, cjmul(u[k], u[3 + k]));
+          }
+        dev = fmax(dev, fabs(n0 - 1.0));
+        dev = fmax(dev, fabs(n1 - 1.0));
+        dev = fmax(dev, fabs(d01.re) + fabs(d01.im));
+      }
+    // max-reduction through the generic sum reducer: reduce exp-free via a
+    // per-block max written as partial; the last block takes the max
+    __shared__ double sh[8];
+    __shared__ bool last;
+    for (int o = 16; o > 0; o >>= 1) dev = fmax(dev, __shfl_xor_sync(0xffffffffu, dev, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = dev;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      {
+        double m = 0;
+        for (int w = 0; w < (int)(blockDim.x / 32); w++) m = fmax(m, sh[w]);
+        red.partial[blockIdx.x] = m;
+        __threadfence();
+        last = (atomicAdd(red.counter, 1u) == gridDim.x - 1);
+      }
+    __syncthreads();
+    if (last && threadIdx.x == 0)
+      {
+        __threadfence();
+        double m = 0;
+        for (int b = 0; b < (int)gridDim.x; b++) m = fmax(m, ((volatile double*)red.partial)[b]);
+        *red.result = m;
+        *red.counter = 0u;
+      }
+  }
+
+  static __global__ void lx_of_eo_kernel(Lattice g, int* __restrict__ out)
+  {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= g.V) return;
+    const int p = idx >= g.Vh, ieo = idx - (p ? (int)g.Vh : 0);
+    out[idx] = eo_site(g, p, ieo).lx;
+  }
+
+  template <int MU, bool UP>
+  __device__ inline int nbr(const Lattice& g, const Site& s)
+  {
+    bool w;
+    return UP ? nbr_up<MU>(g, s, w) : nbr_dw<MU>(g, s, w);
+  }
+
+  static __global__ void geometry_tables_kernel(Lattice g, int* parity, int* eo_of_lx, int* lx_of_eo, int* nup, int* ndw)
+  {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= g.V) return;
+    const int p = idx >= g.Vh, ieo = idx - (p ? (int)g.Vh : 0);
+    const Site s = eo_site(g, p, ieo);
+    parity[s.lx] = p;
+    eo_of_lx[s.lx] = ieo;
+    lx_of_eo[idx] = s.lx;
+    nup[idx * 4 + 0] = nbr<0, true>(g, s);
+    nup[idx * 4 + 1] = nbr<1, true>(g, s);
+    nup[idx * 4 + 2] = nbr<2, true>(g, s);
+    nup[idx * 4 + 3] = nbr<3, true>(g, s);
+    ndw[idx * 4 + 0] = nbr<0, false>(g, s);
+    ndw[idx * 4 + 1] = nbr<1, false>(g, s);
+    ndw[idx * 4 + 2] = nbr<2, false>(g, s);
+    ndw[idx * 4 + 3] = nbr<3, false>(g, s);
+  }
+
+  // out = (1/2k + i sgn mu g5)^(+-1) in
+  template <int P>
+  __global__ void diag_kernel(int n, SpinorT<P> in, SpinorT<P> out, const OpParams* prm, double sgn, int inverse)
+  {
+    using R = typename SpinorT<P>::R;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const C<R> z = inverse ? zinvdiag<R>(*prm, sgn) : zdiag<R>(*prm, sgn);
+    C<R> v[12];
+    in.load(i, v);
+#pragma unroll
+    for (int c = 0; c < 12; c++) v[c] = diag_apply(v[c], z, c);
+    out.store(i, v);
+  }
+
+  // ------------------------------------------------------ spinor transfer
+  // bring an e/o spinor (Vh x 24 doubles, host or device) into a FP64 field
+  inline tms_status spinor_in(tms_ctx* ctx, const double* src, const int* site_map, int64_t nrows, Field& f)
+  {
+    TRY(alloc_field(ctx, f, PREC_F64));
+    const double* d = src;
+    const size_t bytes = (size_t)nrows * 24 * sizeof(double);
+    if (ctx->ptr_mode == TMS_PTR_HOST)
+      {
+        TRY(ensure_stage(ctx, bytes));
+        CU(cudaMemcpyAsync(ctx->stage, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        d = ctx->stage;
+      }
+    const int n = (int)ctx->g.Vh;
+    ++ctx->launches;
+    aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, d, site_map, view<PREC_F64>(f));
+    CU(cudaGetLastError());
+    return TMS_OK;
+  }
+
+  // write a FP64 field out as Vh rows (optionally scattered through site_map) of 24 doubles
+  inline tms_status spinor_out(tms_ctx* ctx, const Field& f, const int* site_map, int64_t nrows, double* dst, bool flush)
+  {
+    const size_t bytes = (size_t)nrows * 24 * sizeof(double);
+    double* d = dst;
+    if (ctx->ptr_mode == TMS_PTR_HOST)
+      {
+        TRY(ensure_stage(ctx, bytes));
+        d = ctx->stage;
+      }
+    const int n = (int)ctx->g.Vh;
+    ++ctx->launches;
+    soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, view<PREC_F64>(f), site_map, d);
+    CU(cudaGetLastError());
+    if (ctx->ptr_mode == TMS_PTR_HOST && flush)
+      {
+        CU(cudaMemcpyAsync(dst, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+      }
+    return TMS_OK;
+  }
+
+  inline tms_status finish(tms_ctx* ctx)
+  {
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(ctx->stream));
+    return TMS_OK;
+  }
+
+  inline tms_status check_conf(tms_ctx* ctx)
+  {
+    if (!ctx) return TMS_ERR_BAD_ARG;
+    if (!ctx->conf_loaded) return fail(ctx, TMS_ERR_NO_CONF, "no gauge configuration uploaded");
+    CU(cudaSetDevice(ctx->device));
+    return TMS_OK;
+  }
+
+  inline double read_result(tms_ctx* ctx)
+  {
+    cudaMemcpyAsync(ctx->red_h, ctx->red_result, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return *ctx->red_h;
+  }
+
+  // the parity-p half of a full-lattice field
+  template <int P>
+  SpinorT<P> view_par(const Field& f, int p)
+  {
+    SpinorT<P> s = view<P>(f);
+    const size_t off = (size_t)p * (size_t)(f.stride / 2);
+    s.d += off;
+    if (s.n) s.n += off;
+    return s;
+  }
+
+  template <int P, int LF, class Epi, class Fin = NoFin>
+  void launch_hop_v(tms_ctx* c, cudaStream_t s, int par_out, int npar, const SpinorT<P>& in_e,
+                    const SpinorT<P>& in_o, const LinkT<LF>& U, const OpParams* prm, const Epi& epi,
+                    const Fin& fin = Fin{}, const int* stop = nullptr)
+  {
+    const int nsite = (int)(npar * c->g.Vh);
+    ++c->launches;
+    hop_kernel<P, LF, Epi, Fin><<<div_up(nsite, HOP_THREADS), HOP_THREADS, 0, s>>>(c->g, par_out, npar, in_e, in_o,
+                                                                                  U, prm, epi, reducer(c), fin, stop);
+  }
+
+  // lx AoS spinor (V rows of 24 doubles, host or device) <-> full-lattice FP64 field
+  inline tms_status lx_in(tms_ctx* ctx, const double* src, Field& full)
+  {
+    TRY(alloc_field(ctx, full, PREC_F64, 2 * ctx->g.stride));
+    const int64_t Vh = ctx->g.Vh;
+    const int n = (int)Vh;
+    const double* d = src;
+    if (ctx->ptr_mode == TMS_PTR_HOST)
+      {
+        const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
+        TRY(ensure_stage(ctx, bytes));
+        CU(cudaMemcpyAsync(ctx->stage, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        d = ctx->stage;
+      }
+    for (int p = 0; p < 2; p++)
+      {
+        ++ctx->launches;
+        aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, d, ctx->lx_of_eo + p * Vh,
+                                                                             view_par<PREC_F64>(full, p));
+      }
+    CU(cudaGetLastError());
+    return TMS_OK;
+  }
+
+  inline tms_status lx_out(tms_ctx* ctx, const Field& full, double* dst)
+  {
+    const int64_t Vh = ctx->g.Vh;
+    const int n = (int)Vh;
+    const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
+    double* d = dst;
+    if (ctx->ptr_mode == TMS_PTR_HOST)
+      {
+        TRY(ensure_stage(ctx, bytes));
+        d = ctx->stage;
+      }
+    for (int p = 0; p < 2; p++)
+      {
+        ++ctx->launches;
+        soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, view_par<PREC_F64>(full, p),
+                                                                             ctx->lx_of_eo + p * Vh, d);
+      }
+    CU(cudaGetLastError());
+    if (ctx->ptr_mode == TMS_PTR_HOST)
+      {
+        CU(cudaMemcpyAsync(dst, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+      }
+    return TMS_OK;
+  }
+
+  template <int P>
+  tms_status norm2(tms_ctx* ctx, const Field& a, double* out, int nsites = 0)
+  {
+    const int n = nsites ? nsites : (int)ctx->g.Vh;
+    ++ctx->launches;
+    norm_kernel<P, false><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, view<P>(a), view<P>(a),
+                                                                                      reducer(ctx));
+    CU(cudaGetLastError());
+    *out = read_result(ctx);
+    return TMS_OK;
+  }
+
+  // ------------------------------------------------------ K operators FP64
+  // out = K(sgn mu) in  (odd -> odd), te is the even temporary
+  template <int P, int LF>
+  void kern_op(tms_ctx* c, const LinkT<LF>& U, const Field& in, const Field& te, const Field& out, double sgn,
+               const OpParams* prm)
+  {
+    EpiInvDiag<P> ea{{view<P>(te), view<P>(te)}, prm, sgn};
+    launch_hop<P, LF>(c, c->stream, 0, 1, in, in, U, prm, ea);
+    EpiKern<P, false> eb{{view<P>(out), view<P>(out)}, {view<P>(in), view<P>(in)}, prm, sgn};
+    launch_hop<P, LF>(c, c->stream, 1, 1, te, te, U, prm, eb);
+  }
+
+
+  inline tms_status push_state(tms_ctx* ctx)
+  {
+    CU(cudaMemcpyAsync(ctx->st, ctx->st_h, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
+    return TMS_OK;
+  }
+  inline tms_status pull_state(tms_ctx* ctx)
+  {
+    CU(cudaMemcpyAsync(ctx->st_h, ctx->st, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return TMS_OK;
+  }
+
+  template <int PD, int PS>
+  void convert(tms_ctx* c, const Field& src, const Field& dst, double a = 1.0, int nsites = 0)
+  {
+    const int n = nsites ? nsites : (int)c->g.Vh;
+    ++c->launches;
+    axpby_kernel<PD, PS, PS><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, c->stream>>>(n, a, view<PS>(src), 0.0,
+                                                                                       view<PS>(src), view<PD>(dst));
+  }
+
+
+}
+

@@ -481,6 +481,223 @@ namespace tms
     }
   };
 
+  // Second half of Q(+mu)Q(-mu) on the full lattice fused with the CG update
+  // (both parities in one launch):  s = Q(+mu) t ;  x += alpha p ;
+  // r -= alpha s ; reduce |r|^2.  The first half is EpiTmQ<P, true>, whose
+  // |Q(-mu) p|^2 = (p, Q(+mu)Q(-mu) p) gives alpha (Q(-mu)^+ = Q(+mu)).
+  template <int P, int PX>
+  struct EpiTmQCgUpdate
+  {
+    static constexpr bool kReduce = true;
+    SpinorT<P> t[2], r[2], p[2];
+    SpinorT<PX> x[2];
+    const OpParams* prm;
+    const CgState* st;
+    double sgn;
+    __device__ __forceinline__ double operator()(int par, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      using RX = typename SpinorT<PX>::R;
+      const R kcf = R(1.0 / (2.0 * prm->kappa)), m = R(sgn * prm->mu);
+      const R alpha = R(st->alpha);
+      C<R> v[12];
+      pick(t[0], t[1], par).load(ieo, v);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> im = {-m * v[c].im, m * v[c].re};
+          const C<R> h = cscale(acc[c], R(0.5));
+          const C<R> k = cscale(v[c], kcf);
+          acc[c] = (c < 6) ? cadd(csub(k, h), im) : cadd(csub(h, k), im); // s
+        }
+      const SpinorT<P> rr = pick(r[0], r[1], par);
+      rr.load(ieo, v);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          v[c] = csub(v[c], cscale(acc[c], alpha));
+          n2 += (double)v[c].re * v[c].re + (double)v[c].im * v[c].im;
+        }
+      rr.store(ieo, v);
+      pick(p[0], p[1], par).load(ieo, v);
+      const SpinorT<PX> xx = pick(x[0], x[1], par);
+      C<RX> xv[12];
+      xx.load(ieo, xv);
+      const RX ax = RX(st->alpha);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          xv[c].re += ax * RX(v[c].re);
+          xv[c].im += ax * RX(v[c].im);
+        }
+      xx.store(ieo, xv);
+      return n2;
+    }
+  };
+
+  // ----------------------------------------------------- multi-shift CGM
+  // cgm_invert, inverters/templates/cgm_invert_template_threaded.hpp:11-295,
+  // with one operator application s = Q_W^2 p per iteration split in two
+  // launches (t = Q_W p reducing |t|^2 = (p, Q_W^2 p); s = Q_W t fused with
+  // r += betaa s reducing |r|^2) and one fused update of p and of every
+  // running shift's solution and direction.
+  constexpr int CGM_MAX_SHIFTS = 32;
+
+  struct CgmState
+  {
+    double rr, b2, betaa, betap, alpha, pap;
+    int iter, niter_max, nshift, nrun, stop, go;
+    double sigma[CGM_MAX_SHIFTS], zps[CGM_MAX_SHIFTS], zas[CGM_MAX_SHIFTS], zfs[CGM_MAX_SHIFTS];
+    double betas[CGM_MAX_SHIFTS], alphas[CGM_MAX_SHIFTS], res[CGM_MAX_SHIFTS], target[CGM_MAX_SHIFTS];
+    int run[CGM_MAX_SHIFTS], upd[CGM_MAX_SHIFTS];
+  };
+
+  // after (p, A p): betaa and the per-shift ratios (:110-158)
+  struct FinCgm1
+  {
+    CgmState* st;
+    __device__ void operator()(double pap) const
+    {
+      st->pap = pap;
+      if (!(pap > 0.0) || isnan(pap))
+        {
+          st->stop = STOP_BREAKDOWN;
+          return;
+        }
+      st->betap = st->betaa;
+      st->betaa = -st->rr / pap;
+      for (int i = 0; i < st->nshift; i++)
+        {
+          st->upd[i] = st->run[i];
+          if (!st->run[i]) continue;
+          const double ratio = st->betap / (st->betaa * st->alpha * (1 - st->zas[i] / st->zps[i]) +
+                                            st->betap * (1 - st->sigma[i] * st->betaa));
+          if (isnan(ratio))
+            {
+              st->stop = STOP_BREAKDOWN;
+              return;
+            }
+          st->zfs[i] = st->zas[i] * ratio;
+          st->betas[i] = st->betaa * ratio;
+        }
+      st->go = 1;
+    }
+  };
+
+  // after |r'|^2: alpha, the per-shift alphas and z shifts, residues and
+  // the per-shift stopping test (:164-260)
+  struct FinCgm2
+  {
+    CgmState* st;
+    __device__ void operator()(double rfrf) const
+    {
+      st->alpha = rfrf / st->rr;
+      for (int i = 0; i < st->nshift; i++)
+        if (st->upd[i])
+          {
+            st->alphas[i] = st->alpha * st->zfs[i] * st->betas[i] / (st->zas[i] * st->betaa);
+            st->zps[i] = st->zas[i];
+            st->zas[i] = st->zfs[i];
+          }
+      st->rr = rfrf;
+      st->iter += 1;
+      int nrun = 0;
+      for (int i = 0; i < st->nshift; i++)
+        {
+          if (st->upd[i])
+            {
+              st->res[i] = st->rr * st->zfs[i] * st->zfs[i] / st->b2;
+              if (st->res[i] < st->target[i]) st->run[i] = 0;
+            }
+          nrun += st->run[i];
+        }
+      st->nrun = nrun;
+      if (isnan(rfrf)) st->stop = STOP_BREAKDOWN;
+      else if (nrun == 0) st->stop = STOP_CONVERGED;
+      else if (st->iter >= st->niter_max) st->stop = STOP_MAXITER;
+    }
+  };
+
+  // s = Q_W t fused with r += betaa s, reduce |r|^2
+  template <int P>
+  struct EpiCgm2
+  {
+    static constexpr bool kReduce = true;
+    SpinorT<P> t[2], r[2];
+    const OpParams* prm;
+    const CgmState* st;
+    __device__ __forceinline__ double operator()(int par, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const R kcf = R(1.0 / (2.0 * prm->kappa)), m = R(prm->mu);
+      const R betaa = R(st->betaa);
+      C<R> v[12];
+      pick(t[0], t[1], par).load(ieo, v);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> im = {-m * v[c].im, m * v[c].re};
+          const C<R> h = cscale(acc[c], R(0.5));
+          const C<R> k = cscale(v[c], kcf);
+          acc[c] = (c < 6) ? cadd(csub(k, h), im) : cadd(csub(h, k), im); // s
+        }
+      const SpinorT<P> rr = pick(r[0], r[1], par);
+      rr.load(ieo, v);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          v[c] = cadd(v[c], cscale(acc[c], betaa));
+          n2 += (double)v[c].re * v[c].re + (double)v[c].im * v[c].im;
+        }
+      rr.store(ieo, v);
+      return n2;
+    }
+  };
+
+  // opens an iteration: the update kernel of the previous one may not run again
+  static __global__ void cgm_begin_kernel(CgmState* st) { st->go = 0; }
+
+  // p = r + alpha p ; for every shift updated this iteration:
+  // sol_i -= betas_i ps_i ; ps_i = zfs_i r + alphas_i ps_i   (:150-158, :185-228)
+  template <int P>
+  __global__ void __launch_bounds__(256)
+    cgm_update_kernel(int n, SpinorT<P> r, SpinorT<P> p, SpinorT<P> x0, SpinorT<P> ps0, size_t shift_elems,
+                      const CgmState* __restrict__ st)
+  {
+    using R = typename SpinorT<P>::R;
+    if (!st->go) return;
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    C<R> rv[12], v[12], w[12];
+    r.load(i, rv);
+    p.load(i, v);
+    const R alpha = R(st->alpha);
+#pragma unroll
+    for (int c = 0; c < 12; c++) v[c] = cadd(rv[c], cscale(v[c], alpha));
+    p.store(i, v);
+    const int ns = st->nshift;
+    for (int k = 0; k < ns; k++)
+      {
+        if (!st->upd[k]) continue;
+        SpinorT<P> xk = x0, pk = ps0;
+        xk.d += k * shift_elems;
+        pk.d += k * shift_elems;
+        if (xk.n) xk.n += k * (size_t)x0.stride;
+        if (pk.n) pk.n += k * (size_t)ps0.stride;
+        const R bs = R(st->betas[k]), z = R(st->zfs[k]), as = R(st->alphas[k]);
+        pk.load(i, v);
+        xk.load(i, w);
+#pragma unroll
+        for (int c = 0; c < 12; c++) w[c] = csub(w[c], cscale(v[c], bs));
+        xk.store(i, w);
+#pragma unroll
+        for (int c = 0; c < 12; c++) v[c] = cadd(cscale(rv[c], z), cscale(v[c], as));
+        pk.store(i, v);
+      }
+  }
+
   // ---------------------------------------------------------- hop kernel
   // Launch: one thread per output site; npar = 1 computes the parity
   // par_out only, npar = 2 both parities (grid over 2*Vh).

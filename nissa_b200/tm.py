@@ -226,6 +226,45 @@ class Lattice:
             self._check(st, "inv_tmDkern_eoprec_square_eos_cg", stats.as_dict(), sol)
         return sol, stats.as_dict()
 
+    def inv_tmQ2_cg(self, kappa, m, source_lx, niter, residue, guess=None, anis=None, precision="double", out=None,
+                    raise_on_error=True):
+        """Full-lattice CG on Q(+m)Q(-m) (lx spinors).  Returns (sol, stats)."""
+        shape = (self.V, 4, 3, 2)
+        s, g = _Buf(source_lx, shape), _Buf(guess, shape)
+        sol = self._new_out(source_lx, shape) if out is None else out
+        o = _Buf(sol, shape, out=True)
+        self._mode(s, g, o)
+        stats = _lib.Stats()
+        a = self._anis(anis)
+        st = self.lib.tms_cg_tmQ2(self.h, o.ptr, g.ptr, s.ptr, kappa, a[0], a[1], m, int(niter), float(residue),
+                                  PRECISION[precision], ctypes.byref(stats))
+        if raise_on_error:
+            self._check(st, "inv_tmQ2_cg", stats.as_dict(), sol)
+        return sol, stats.as_dict()
+
+    def inv_tmQ2_cgm(self, kappa, masses, source_lx, niter, residues, anis=None, precision="double", out=None,
+                     raise_on_error=True):
+        """Multi-shift CG: (Q_W^2 + m_k^2) sol_k = source for every mass.  Returns (sols, [stats])."""
+        shape = (self.V, 4, 3, 2)
+        nm = len(masses)
+        residues = np.broadcast_to(np.asarray(residues, np.float64), (nm,)).copy()
+        masses = np.ascontiguousarray(masses, np.float64)
+        s = _Buf(source_lx, shape)
+        if out is None:
+            out = [self._new_out(source_lx, shape) for _ in range(nm)]
+        obufs = [_Buf(o, shape, out=True) for o in out]
+        self._mode(s, *obufs)
+        ptrs = (ctypes.c_void_p * nm)(*[b.ptr for b in obufs])
+        stats = (_lib.Stats * nm)()
+        a = self._anis(anis)
+        st = self.lib.tms_cgm_tmQ2(self.h, ctypes.cast(ptrs, ctypes.c_void_p), s.ptr, kappa, a[0], a[1],
+                                   masses.ctypes.data, nm, int(niter), residues.ctypes.data, PRECISION[precision],
+                                   ctypes.cast(stats, ctypes.c_void_p))
+        sd = [x.as_dict() for x in stats]
+        if raise_on_error:
+            self._check(st, "inv_tmQ2_cgm", sd, out)
+        return out, sd
+
     def inv_tmD_cg_eoprec(self, kappa, mu, source_lx, niter, residue, anis=None, precision="double", out=None,
                           raise_on_error=True):
         """Full solve D_tm sol = source (lx spinors) via e/o preconditioning.  Returns (sol, stats)."""
