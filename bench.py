@@ -327,9 +327,15 @@ def run_kernel_only(args):
     conf = wl.gauge_conf(W["T"], W["L"], W["eps"], W["seed"], device="cuda:0")
     lat = Lattice(W["T"], W["L"], bc_t=W["bc_t"])
     lat.upload_conf(conf)
-    ms, by = lat.bench_hop(args.kernel_only, variant=args.variant, nrep=args.nrep, flush=True)
+    if args.nrhs > 1:
+        if args.mrhs:
+            lat.set_tuning("mrhs_per_thread", args.mrhs)
+        ms, by = lat.bench_hop_batched(args.kernel_only, nrhs=args.nrhs, nrep=args.nrep, flush=True)
+    else:
+        ms, by = lat.bench_hop(args.kernel_only, variant=args.variant, nrep=args.nrep, flush=True)
     torch.cuda.synchronize()
-    print(json.dumps({"kernel": "hop", "precision": args.kernel_only, "variant": args.variant, "T": W["T"],
+    print(json.dumps({"kernel": "hop", "precision": args.kernel_only, "variant": args.variant, "nrhs": args.nrhs,
+                      "T": W["T"],
                       "L": W["L"], "ms_per_launch": ms, "alg_bytes_per_launch": by,
                       "achieved_gbs": by / (ms * 1e-3) / 1e9}), flush=True)
 
@@ -392,6 +398,8 @@ def main():
                     help="only time the e/o hopping kernel of this precision (profiling entry point)")
     ap.add_argument("--variant", type=int, default=1, help="hopping kernel variant for --kernel-only")
     ap.add_argument("--nrep", type=int, default=10, help="launches for --kernel-only")
+    ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
+    ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
     ap.add_argument("--workload", default="cg", choices=["cg", "cgm"],
                     help="cg: the headline solve; cgm: the multi-shift workload (extra report)")
     ap.add_argument("--cgm-precision", default="single", choices=["single", "half"])

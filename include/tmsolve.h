@@ -149,10 +149,28 @@ tms_status tms_cgm_tmQ2(tms_ctx *ctx, double *const *sols, const double *src_lx,
                         double anis, const double *masses, int nmass, int niter, const double *residues,
                         int precision, tms_stats *stats);
 
+/* Batched inv_tmD_cg_eoprec (the reference solves one right-hand side per call,
+ * inverters/twisted_mass/cg_invert_tmD_eoprec.cpp:152-213): nrhs (<= 64) lx sources with one kappa
+ * and a twisted mass mus[k] each; the e/o CG of all of them runs in lock step so that each hop reads
+ * the links once for every right-hand side.  Each right-hand side stops at its own residues[k]
+ * (squared, relative); the FP64 reliable updates of the mixed precisions are per right-hand side.
+ * sols_lx/srcs_lx are arrays of nrhs lx spinors; stats (may be NULL) receives nrhs entries. */
+tms_status tms_cg_eoprec_batched(tms_ctx *ctx, int nrhs, double *const *sols_lx, const double *const *srcs_lx,
+                                 double kappa, int has_anis, double anis, const double *mus, int niter,
+                                 const double *residues, int precision, tms_stats *stats);
+
 /* ---- instrumentation (no reference counterpart) ---- */
 
 /* Number of CUDA kernels this context has launched (CUDA-graph replays count their nodes). */
 uint64_t tms_launch_count(const tms_ctx *ctx);
+/* Tuning knobs (no reference counterpart), used by the autotuner: "hop_cfg_double",
+ * "hop_cfg_single", "hop_cfg_half" (hopping-kernel launch shape 0..2: 128 threads; 128 threads
+ * with registers capped for 4 (FP64) / 8 resident blocks; 256 threads capped for 2 / 4),
+ * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
+ * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
+ * dropped by this factor, 0 < delta < 1), "mrhs_per_thread" (right-hand sides one thread of the
+ * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2).  Results do not depend on the launch shapes. */
+tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);
 /* Time the e/o hopping kernel alone with CUDA events on the context's stream: nrep launches,
  * each preceded (untimed) by a 512 MiB write that flushes the L2 when flush=1.
  * precision: tms_precision; variant 0 plain hop, 1 hop + inverse diagonal (CG first half),
@@ -161,6 +179,11 @@ uint64_t tms_launch_count(const tms_ctx *ctx);
  * Vh x (8 links + input spinor + output spinor [+ own-site spinor for variant 2]). */
 tms_status tms_bench_hop(tms_ctx *ctx, int precision, int variant, int nrep, int flush, double *ms_per_launch,
                          double *bytes_per_launch);
+
+/* tms_bench_hop for the batched (multi-RHS) hopping kernel with the inverse-diagonal epilogue:
+ * nrhs right-hand sides per launch; algorithmic bytes = Vh x (8 links + 2 nrhs spinors). */
+tms_status tms_bench_hop_batched(tms_ctx *ctx, int precision, int nrhs, int nrep, int flush, double *ms_per_launch,
+                                 double *bytes_per_launch);
 
 /* ---- allocation-free hopping (no counterpart in the reference) ---- */
 

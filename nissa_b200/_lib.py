@@ -44,8 +44,11 @@ SIGNATURES = {
     "tms_cg_eoprec": (I, [P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cg_tmQ2": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cgm_tmQ2": (I, [P, P, P, D, I, D, P, I, I, P, I, P]),
+    "tms_cg_eoprec_batched": (I, [P, I, P, P, D, I, D, P, I, P, I, P]),
     "tms_launch_count": (ctypes.c_uint64, [P]),
+    "tms_set_tuning": (I, [P, ctypes.c_char_p, D]),
     "tms_bench_hop": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),
+    "tms_bench_hop_batched": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),
     "tms_hop_eo_noalloc": (I, [I, I, D, P, I, I, I, P, P, I, D, P, ctypes.c_char_p, I]),
 }
 

@@ -43,14 +43,28 @@ def nvcc() -> str:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every .cu of csrc/ to an object in parallel, then link the shared library."""
     if not force and not stale():
         return LIB
-    tmp = LIB + ".tmp%d" % os.getpid()
-    cmd = [nvcc()] + NVCC_FLAGS + ["-I" + INCLUDE, "-I" + CSRC] + sources() + ["-o", tmp]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.check_call(cmd)
-    os.replace(tmp, LIB)
+    import concurrent.futures
+    import tempfile
+    with tempfile.TemporaryDirectory(prefix="tms_build_") as d:
+        objs = []
+        cmds = []
+        for src in sources():
+            obj = os.path.join(d, os.path.basename(src) + ".o")
+            objs.append(obj)
+            cmds.append([nvcc()] + [f for f in NVCC_FLAGS if f != "-shared"] + ["-I" + INCLUDE, "-I" + CSRC, "-c", src,
+                                                                               "-o", obj])
+        with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+            for cmd, rc in zip(cmds, ex.map(lambda c: subprocess.call(c), cmds)):
+                if verbose:
+                    print(" ".join(cmd))
+                if rc != 0:
+                    raise subprocess.CalledProcessError(rc, cmd)
+        tmp = LIB + ".tmp%d" % os.getpid()
+        subprocess.check_call([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + objs + ["-o", tmp])
+        os.replace(tmp, LIB)
     return LIB
 
 

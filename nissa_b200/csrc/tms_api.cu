@@ -142,6 +142,7 @@ tms_status tms_destroy(tms_ctx* ctx)
   for (auto& f : ctx->f64) { fr(f.d); fr(f.n); }
   for (auto& f : ctx->lo) { fr(f.d); fr(f.n); }
   for (auto& f : ctx->ex) { fr(f.d); fr(f.n); }
+  if (ctx->bw && ctx->bw_free) ctx->bw_free(ctx->bw);
   for (auto& f : ctx->lx64) { fr(f.d); fr(f.n); }
   for (auto& f : ctx->lxlo) { fr(f.d); fr(f.n); }
   fr(ctx->lxxlo.d);
@@ -156,6 +157,7 @@ tms_status tms_destroy(tms_ctx* ctx)
   fr(ctx->U64);
   fr(ctx->U32r);
   fr(ctx->U32f);
+  fr(ctx->U16r);
   fr(ctx->prm);
   fr(ctx->st);
   fr(ctx->red_partial);
@@ -212,6 +214,7 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
   if (!ctx->U64) CU(cudaMalloc(&ctx->U64, (size_t)V * 36 * sizeof(double2)));
   if (!ctx->U32r) CU(cudaMalloc(&ctx->U32r, (size_t)V * 12 * sizeof(float4)));
   if (!ctx->U32f) CU(cudaMalloc(&ctx->U32f, (size_t)V * 36 * sizeof(float2)));
+  if (!ctx->U16r) CU(cudaMalloc(&ctx->U16r, (size_t)V * 12 * sizeof(short4)));
   const double* src = conf;
   if (ctx->ptr_mode == TMS_PTR_HOST)
     {
@@ -225,7 +228,7 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
   CU(cudaGetLastError());
   const int64_t nl = 8 * Vh;
   ++ctx->launches;
-  conf_lowprec_kernel<<<div_up(nl, 256), 256, 0, ctx->stream>>>(nl, (int)Vh, ctx->U64, ctx->U32r, ctx->U32f,
+  conf_lowprec_kernel<<<div_up(nl, 256), 256, 0, ctx->stream>>>(nl, (int)Vh, ctx->U64, ctx->U32r, ctx->U32f, ctx->U16r,
                                                                  reducer(ctx));
   CU(cudaGetLastError());
   const double dev = read_result(ctx);
@@ -377,6 +380,58 @@ tms_status tms_apply_tmQ2(tms_ctx* ctx, double kappa, int has_anis, double anis,
 
 uint64_t tms_launch_count(const tms_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
+{
+  if (!ctx || !key) return TMS_ERR_BAD_ARG;
+  const std::string k = key;
+  auto drop_all = [&]() {
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& g : ctx->graph)
+      if (g)
+        {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+  };
+  if (k == "hop_cfg_double" || k == "hop_cfg_single" || k == "hop_cfg_half")
+    {
+      const int v = (int)value;
+      if (v < 0 || v >= HOP_CFGS || v != value) return fail(ctx, TMS_ERR_BAD_ARG, "%s: 0..%d", key, HOP_CFGS - 1);
+      const int p = (k == "hop_cfg_double") ? PREC_F64 : (k == "hop_cfg_single") ? PREC_F32 : PREC_F16;
+      if (ctx->hop_cfg[p] != v) drop_all();
+      ctx->hop_cfg[p] = v;
+      return TMS_OK;
+    }
+  if (k == "graph_iters")
+    {
+      const int v = (int)value;
+      if (v < 1 || v > 64 || v != value) return fail(ctx, TMS_ERR_BAD_ARG, "graph_iters: 1..64");
+      if (ctx->graph_iters != v) drop_all();
+      ctx->graph_iters = v;
+      return TMS_OK;
+    }
+  if (k == "mrhs_per_thread")
+    {
+      const int v = (int)value;
+      if (v != 1 && v != 2 && v != 4) return fail(ctx, TMS_ERR_BAD_ARG, "mrhs_per_thread: 1, 2 or 4");
+      if (ctx->mrhs_r != v && ctx->bw && ctx->bw_free)
+        {
+          cudaStreamSynchronize(ctx->stream);
+          ctx->bw_free(ctx->bw); // its graphs were captured with the old shape
+          ctx->bw = nullptr;
+        }
+      ctx->mrhs_r = v;
+      return TMS_OK;
+    }
+  if (k == "reliable_delta_single" || k == "reliable_delta_half")
+    {
+      if (!(value > 0.0 && value < 1.0)) return fail(ctx, TMS_ERR_BAD_ARG, "%s: in (0, 1)", key);
+      (k == "reliable_delta_single" ? ctx->delta_single : ctx->delta_half) = value;
+      return TMS_OK;
+    }
+  return fail(ctx, TMS_ERR_BAD_ARG, "unknown tuning key %s", key);
+}
+
 tms_status tms_bench_hop(tms_ctx* ctx, int precision, int variant, int nrep, int flush, double* ms_per_launch,
                          double* bytes_per_launch)
 {
@@ -393,7 +448,7 @@ tms_status tms_bench_hop(tms_ctx* ctx, int precision, int variant, int nrep, int
                     : bench_hop_t<PREC_F32>(ctx, links32f(ctx), variant, nrep, flush, ms_per_launch, 72.0, 96.0,
                                             bytes_per_launch);
   if (precision == TMS_PREC_MIXED_HALF)
-    return ctx->su3 ? bench_hop_t<PREC_F16>(ctx, links32r(ctx), variant, nrep, flush, ms_per_launch, 48.0, 52.0,
+    return ctx->su3 ? bench_hop_t<PREC_F16>(ctx, links16r(ctx), variant, nrep, flush, ms_per_launch, 24.0, 52.0,
                                             bytes_per_launch)
                     : bench_hop_t<PREC_F16>(ctx, links32f(ctx), variant, nrep, flush, ms_per_launch, 72.0, 52.0,
                                             bytes_per_launch);

@@ -1,0 +1,409 @@
+// Multi-RHS kernels: k right-hand sides, each with its own twisted mass and
+// its own CG scalars, share one pass over the gauge links.
+//
+// Launch shape: persistent blocks of 8 warps walk the lattice 32 sites at a
+// time; for each 32-site chunk warp w takes the right-hand sides w, w+8, ...
+// All warps of a block read the same links for the same sites, so the links
+// cross HBM about once per chunk and are served to the other right-hand sides
+// from L1; each right-hand side's spinors are read by one warp as contiguous
+// 128-bit segments.
+//
+// Reductions are per right-hand side: a block accumulates each right-hand
+// side's warp sums in shared memory, writes one partial per block, and the
+// warp that takes the last ticket of that right-hand side sums the row in a
+// fixed order and finalises its scalars (no warp ever waits).
+#pragma once
+
+#include "tms_kernels.cuh"
+
+namespace tms
+{
+  constexpr int MRHS_MAX = 64;
+
+  // k fields of one precision laid out one after the other
+  template <int P>
+  struct SpinorBatch
+  {
+    SpinorT<P> f;       // right-hand side 0
+    size_t rhs_elems;   // element offset between right-hand sides (d)
+    size_t rhs_norms;   // float offset between right-hand sides (n, FP16 only)
+    __device__ __forceinline__ SpinorT<P> rhs(int r) const
+    {
+      SpinorT<P> s = f;
+      s.d += (size_t)r * rhs_elems;
+      if (s.n) s.n += (size_t)r * rhs_norms;
+      return s;
+    }
+  };
+
+  struct BatchParams
+  {
+    double kappa, anis;
+    double mu[MRHS_MAX];
+  };
+
+  struct BatchReducer
+  {
+    double* partial;    // [rhs][gridDim.x]
+    unsigned* counter;  // [rhs]
+    double* result;     // [rhs]
+  };
+
+  // finish the reduction of right-hand side `rhs`: lane 0 holds this block's
+  // partial; the warp holding the last ticket of that right-hand side sums the
+  // row in a fixed order and calls fin(rhs, total)
+  template <class Fin>
+  __device__ __forceinline__ void warp_rhs_finish(double v, int rhs, const BatchReducer& red, const Fin& fin)
+  {
+    const int lane = threadIdx.x & 31;
+    unsigned last = 0;
+    if (lane == 0)
+      {
+        red.partial[(size_t)rhs * gridDim.x + blockIdx.x] = v;
+        __threadfence();
+        last = (atomicAdd(red.counter + rhs, 1u) == gridDim.x - 1);
+      }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    double s = 0.0;
+    const volatile double* row = red.partial + (size_t)rhs * gridDim.x;
+    for (int i = lane; i < (int)gridDim.x; i += 32) s += row[i];
+    s = warp_sum(s);
+    if (lane == 0)
+      {
+        red.result[rhs] = s;
+        red.counter[rhs] = 0u;
+        fin(rhs, s);
+      }
+  }
+
+  struct NoFinB
+  {
+    __device__ void operator()(int, double) const {}
+  };
+
+  // per right-hand side: alpha = rr / |K(-mu) p|^2
+  struct FinAlphaB
+  {
+    CgState* st;
+    __device__ void operator()(int r, double pAp) const { FinAlpha{st + r}(pAp); }
+  };
+  struct FinBetaB
+  {
+    CgState* st;
+    __device__ void operator()(int r, double rr) const { FinBeta{st + r}(rr); }
+  };
+
+  // ------------------------------------------------------------ epilogues
+  template <int P>
+  struct EpiBInvDiag
+  {
+    static constexpr bool kReduce = false;
+    SpinorBatch<P> out;
+    double sgn;
+    __device__ __forceinline__ double operator()(int r, int ieo, const BatchParams& bp,
+                                                 C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const OpParams o{bp.kappa, bp.mu[r], bp.anis};
+      const C<R> z = zinvdiag<R>(o, sgn);
+#pragma unroll
+      for (int c = 0; c < 12; c++) acc[c] = diag_apply(acc[c], z, c);
+      out.rhs(r).store(ieo, acc);
+      return 0.0;
+    }
+  };
+
+  template <int P, bool RED>
+  struct EpiBKern
+  {
+    static constexpr bool kReduce = RED;
+    SpinorBatch<P> out, x;
+    double sgn;
+    __device__ __forceinline__ double operator()(int r, int ieo, const BatchParams& bp,
+                                                 C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const OpParams o{bp.kappa, bp.mu[r], bp.anis};
+      const C<R> z = zdiag<R>(o, sgn);
+      C<R> xv[12];
+      x.rhs(r).load(ieo, xv);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> d = diag_apply(xv[c], z, c);
+          const C<R> q = cscale(acc[c], R(0.25));
+          acc[c] = (c < 6) ? csub(d, q) : csub(q, d);
+          if (RED) n2 += (double)acc[c].re * acc[c].re + (double)acc[c].im * acc[c].im;
+        }
+      out.rhs(r).store(ieo, acc);
+      return n2;
+    }
+  };
+
+  // s = K(+mu) t1 ; x += alpha p ; r -= alpha s ; reduce |r|^2 (per right-hand side)
+  template <int P, int PX>
+  struct EpiBKernCgUpdate
+  {
+    static constexpr bool kReduce = true;
+    SpinorBatch<P> t1, r, p;
+    SpinorBatch<PX> x;
+    const CgState* st;
+    double sgn;
+    __device__ __forceinline__ double operator()(int k, int ieo, const BatchParams& bp,
+                                                 C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      using RX = typename SpinorT<PX>::R;
+      const OpParams o{bp.kappa, bp.mu[k], bp.anis};
+      const C<R> z = zdiag<R>(o, sgn);
+      const double a = st[k].alpha;
+      const R alpha = R(a);
+      C<R> v[12];
+      t1.rhs(k).load(ieo, v);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> d = diag_apply(v[c], z, c);
+          const C<R> q = cscale(acc[c], R(0.25));
+          acc[c] = (c < 6) ? csub(d, q) : csub(q, d);
+        }
+      const SpinorT<P> rk = r.rhs(k);
+      rk.load(ieo, v);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          v[c] = csub(v[c], cscale(acc[c], alpha));
+          n2 += (double)v[c].re * v[c].re + (double)v[c].im * v[c].im;
+        }
+      rk.store(ieo, v);
+      p.rhs(k).load(ieo, v);
+      const SpinorT<PX> xk = x.rhs(k);
+      C<RX> xv[12];
+      xk.load(ieo, xv);
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          xv[c].re += RX(a) * RX(v[c].re);
+          xv[c].im += RX(a) * RX(v[c].im);
+        }
+      xk.store(ieo, xv);
+      return n2;
+    }
+  };
+
+  // ---------------------------------------------------------- hop kernel
+  // One parity (par_out) for nrhs right-hand sides, register-blocked: a
+  // thread computes one site for R right-hand sides at once, so each link is
+  // loaded (and rebuilt) once into registers and applied to the R neighbour
+  // spinors.  A warp takes 32 consecutive sites and the groups of R
+  // right-hand sides one after the other (the links of its sites stay in L1
+  // across groups).
+  // A right-hand side whose state says stop is skipped.  Per right-hand side
+  // sums are reduced with warp shuffles, kept per warp in shared memory and
+  // combined in a fixed order: deterministic.
+  constexpr int MRHS_WARPS = 4;
+
+  template <int MU, bool FWD, int P, int LF, int R>
+  __device__ __forceinline__ void hop_dir_multi(const Lattice& g, const Site& s, int p, int ieo,
+                                                const SpinorBatch<P>& in, int rhs0, unsigned on, const LinkT<LF>& U,
+                                                typename SpinorT<P>::R anis, C<typename SpinorT<P>::R> acc[R][12])
+  {
+    using Re = typename SpinorT<P>::R;
+    const Re fmu = (MU > 0) ? anis : Re(1);
+    bool w;
+    const int n = FWD ? nbr_up<MU>(g, s, w) : nbr_dw<MU>(g, s, w);
+    C<Re> L[9];
+    U.load(FWD ? p : 1 - p, MU, FWD ? ieo : n, L);
+    const Re f = w ? fmu * Re(g.bc_t) : fmu;
+#pragma unroll
+    for (int j = 0; j < R; j++)
+      if (on & (1u << j))
+        {
+          C<Re> sp[12], h0[3], h1[3], u0[3], u1[3];
+          in.rhs(rhs0 + j).load(n, sp);
+          project<MU, FWD>(sp, h0, h1);
+          link_mul<FWD>(L, h0, u0, f);
+          link_mul<FWD>(L, h1, u1, f);
+          reconstruct<MU, FWD>(acc[j], u0, u1);
+        }
+  }
+
+  // resident blocks the register budget is capped for: more right-hand sides
+  // per thread need more accumulator registers
+  template <int P, int R>
+  struct MrhsMinBlocks
+  {
+    static constexpr int value = (P == PREC_F64) ? (R == 1 ? 3 : 2) : (R == 1 ? 6 : R == 2 ? 4 : 2);
+  };
+
+  template <int P, int LF, class Epi, class Fin, int R>
+  __global__ void __launch_bounds__(MRHS_WARPS * 32, MrhsMinBlocks<P, R>::value)
+    hop_mrhs_kernel(Lattice g, int par_out, int nrhs, SpinorBatch<P> in, LinkT<LF> U, const BatchParams* __restrict__ bp,
+                    Epi epi, BatchReducer red, Fin fin, const CgState* __restrict__ st)
+  {
+    using Re = typename SpinorT<P>::R;
+    __shared__ double sh[Epi::kReduce ? MRHS_WARPS * MRHS_MAX : 1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ngroups = (nrhs + R - 1) / R;
+    if (Epi::kReduce)
+      {
+        for (int i = threadIdx.x; i < MRHS_WARPS * MRHS_MAX; i += blockDim.x) sh[i] = 0.0;
+        __syncthreads();
+      }
+    const Re anis = Re(bp->anis);
+    const int nchunks = (int)((g.Vh + 31) / 32);
+    const int c = blockIdx.x * MRHS_WARPS + w;
+    if (c < nchunks)
+      {
+        const int ieo = c * 32 + lane;
+        for (int gr = 0; gr < ngroups; gr++)
+          {
+            const int rhs0 = gr * R;
+            unsigned on = 0;
+#pragma unroll
+            for (int j = 0; j < R; j++)
+              if (rhs0 + j < nrhs && !(st && st[rhs0 + j].stop)) on |= 1u << j;
+            if (!on) continue; // warp-uniform
+            double part[R];
+#pragma unroll
+            for (int j = 0; j < R; j++) part[j] = 0.0;
+            if (ieo < g.Vh)
+              {
+                C<Re> acc[R][12];
+#pragma unroll
+                for (int j = 0; j < R; j++)
+#pragma unroll
+                  for (int k = 0; k < 12; k++) acc[j][k] = {Re(0), Re(0)};
+                const Site s = eo_site(g, par_out, ieo);
+                hop_dir_multi<0, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                hop_dir_multi<0, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                hop_dir_multi<1, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                hop_dir_multi<1, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                hop_dir_multi<2, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                hop_dir_multi<2, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                hop_dir_multi<3, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                hop_dir_multi<3, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+#pragma unroll
+                for (int j = 0; j < R; j++)
+                  if (on & (1u << j)) part[j] = epi(rhs0 + j, ieo, *bp, acc[j]);
+              }
+            if (Epi::kReduce)
+#pragma unroll
+              for (int j = 0; j < R; j++)
+                if (on & (1u << j))
+                  {
+                    const double v = warp_sum(part[j]);
+                    if (lane == 0) sh[w * MRHS_MAX + rhs0 + j] += v;
+                  }
+          }
+      }
+    if (Epi::kReduce)
+      {
+        __syncthreads();
+        // warp w finishes right-hand sides w, w + MRHS_WARPS, ...
+        for (int rhs = w; rhs < nrhs; rhs += MRHS_WARPS)
+          {
+            if (st && st[rhs].stop) continue;
+            double v = 0.0;
+            if (lane == 0)
+#pragma unroll
+              for (int ww = 0; ww < MRHS_WARPS; ww++) v += sh[ww * MRHS_MAX + rhs];
+            warp_rhs_finish(v, rhs, red, fin);
+          }
+      }
+  }
+
+  // r = b - s and |r|^2 per right-hand side (FP64); grid (blocks, nrhs)
+  static __global__ void __launch_bounds__(256)
+    residual_mrhs_kernel(int n, int nrhs, SpinorBatch<PREC_F64> b, SpinorBatch<PREC_F64> s, SpinorBatch<PREC_F64> r,
+                         BatchReducer red, const CgState* __restrict__ mask)
+  {
+    __shared__ double sh[8];
+    const int k = blockIdx.y;
+    if (k >= nrhs || (mask && mask[k].stop)) return; // whole block
+    const SpinorT<PREC_F64> bk = b.rhs(k), sk = s.rhs(k), rk = r.rhs(k);
+    double acc = 0.0;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+      {
+        C<double> u[12], v[12];
+        bk.load(i, u);
+        sk.load(i, v);
+#pragma unroll
+        for (int c = 0; c < 12; c++)
+          {
+            u[c] = csub(u[c], v[c]);
+            acc += u[c].re * u[c].re + u[c].im * u[c].im;
+          }
+        rk.store(i, u);
+      }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32)
+      {
+        double v = (threadIdx.x < 8) ? sh[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        warp_rhs_finish(v, k, red, NoFinB{});
+      }
+  }
+
+  // out = a x + b y per right-hand side (any precisions), masked
+  template <int PO, int PX, int PY>
+  __global__ void __launch_bounds__(256)
+    axpby_mrhs_kernel(int n, int nrhs, double a, SpinorBatch<PX> x, double b, SpinorBatch<PY> y, SpinorBatch<PO> out,
+                      const CgState* __restrict__ mask)
+  {
+    using RO = typename SpinorT<PO>::R;
+    const int k = blockIdx.y;
+    if (k >= nrhs || (mask && mask[k].stop)) return;
+    const SpinorT<PX> xk = x.rhs(k);
+    const SpinorT<PY> yk = y.rhs(k);
+    const SpinorT<PO> ok = out.rhs(k);
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+      {
+        C<typename SpinorT<PX>::R> u[12];
+        C<typename SpinorT<PY>::R> v[12];
+        C<RO> w[12];
+        xk.load(i, u);
+        if (b != 0.0) yk.load(i, v);
+#pragma unroll
+        for (int c = 0; c < 12; c++)
+          {
+            double re = a * (double)u[c].re, im = a * (double)u[c].im;
+            if (b != 0.0)
+              {
+                re += b * (double)v[c].re;
+                im += b * (double)v[c].im;
+              }
+            w[c] = {RO(re), RO(im)};
+          }
+        ok.store(i, w);
+      }
+  }
+
+  // p = r + beta p per right-hand side
+  template <int P>
+  __global__ void __launch_bounds__(256)
+    xpay_mrhs_kernel(int n, int nrhs, SpinorBatch<P> r, SpinorBatch<P> p, const CgState* __restrict__ st,
+                     const CgState* __restrict__ mask)
+  {
+    using R = typename SpinorT<P>::R;
+    const int k = blockIdx.y;
+    if (k >= nrhs || (mask ? mask[k].stop : st[k].stop)) return;
+    const R beta = R(st[k].beta);
+    const SpinorT<P> rk = r.rhs(k), pk = p.rhs(k);
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+      {
+        C<R> a[12], b[12];
+        rk.load(i, a);
+        pk.load(i, b);
+#pragma unroll
+        for (int c = 0; c < 12; c++) b[c] = cadd(a[c], cscale(b[c], beta));
+        pk.store(i, b);
+      }
+  }
+}

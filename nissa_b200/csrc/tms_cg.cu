@@ -265,7 +265,7 @@ namespace
       }
     Field& xlo = Op::xlo(ctx);
     TRY(alloc_field(ctx, xlo, PX, Op::stride(ctx)));
-    const double delta = (P == PREC_F16) ? 0.1 : 0.05; // reliable-update trigger (residual reduction)
+    const double delta = (P == PREC_F16) ? ctx->delta_half : ctx->delta_single; // reliable-update trigger
     double b2;
     TRY(norm2<PREC_F64>(ctx, f[0], &b2, n));
     if (b2 == 0.0 || std::isnan(b2)) return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm: %g", b2);
@@ -356,7 +356,7 @@ namespace
       return ctx->su3 ? cg_mixed<Op, PREC_F32>(ctx, links32r(ctx), niter, residue, have_guess, stats)
                       : cg_mixed<Op, PREC_F32>(ctx, links32f(ctx), niter, residue, have_guess, stats);
     if (precision == TMS_PREC_MIXED_HALF)
-      return ctx->su3 ? cg_mixed<Op, PREC_F16>(ctx, links32r(ctx), niter, residue, have_guess, stats)
+      return ctx->su3 ? cg_mixed<Op, PREC_F16>(ctx, links16r(ctx), niter, residue, have_guess, stats)
                       : cg_mixed<Op, PREC_F16>(ctx, links32f(ctx), niter, residue, have_guess, stats);
     return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
   }

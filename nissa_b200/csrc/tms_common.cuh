@@ -12,6 +12,8 @@
 //   links,  FP32   float4  U[par][mu][3][Vh]        12 reals: rows 0 and 1; row 2 is
 //                                                   rebuilt as conj(row0 x row1)
 //   links,  FP32   float2  U[par][mu][9][Vh]        18 reals, for non-SU(3) links
+//   links,  I16    short4  U[par][mu][3][Vh]        12 reals in 16-bit fixed point (value/32767;
+//                                                   SU(3) entries are bounded by 1), row 2 rebuilt
 //
 // Sites of one parity are numbered as the reference numbers them
 // (geometry_eo.cpp:66-77): lx = ((t*LX + x)*LY + y)*LZ + z, and the e/o index
@@ -26,7 +28,7 @@
 namespace tms
 {
   enum Prec { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2 };
-  enum LinkFmt { LINK_F64_18 = 0, LINK_F32_12 = 1, LINK_F32_18 = 2 };
+  enum LinkFmt { LINK_F64_18 = 0, LINK_F32_12 = 1, LINK_F32_18 = 2, LINK_I16_12 = 3 };
 
   // ------------------------------------------------------------- geometry
   struct Lattice
@@ -197,8 +199,11 @@ namespace tms
       float m = 0.f;
 #pragma unroll
       for (int c = 0; c < 12; c++) m = fmaxf(m, fmaxf(fabsf(v[c].re), fabsf(v[c].im)));
-      const float inv = (m > 0.f) ? 1.f / m : 0.f;
-      n[site] = m;
+      // a site whose largest component is below 1e-30 is stored as zero (its
+      // inverse would overflow and 0*inf give NaN)
+      const bool live = (m > 1e-30f);
+      const float inv = live ? 1.f / m : 0.f;
+      n[site] = live ? m : 0.f;
 #pragma unroll
       for (int k = 0; k < 3; k++)
         {
@@ -267,6 +272,28 @@ namespace tms
       u[4] = {a2.x, a2.y};
       u[5] = {a2.z, a2.w};
       // row 2 = conj(row0 x row1): exact for special-unitary links
+      u[6] = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
+      u[7] = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));
+      u[8] = cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));
+    }
+  };
+
+  template <> struct LinkT<LINK_I16_12>
+  {
+    using R = float;
+    const short4* __restrict__ d; // [par][mu][3][Vh]
+    int Vh;
+    __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
+    {
+      constexpr float k = 1.0f / 32767.0f;
+      const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
+      const short4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      u[0] = {a0.x * k, a0.y * k};
+      u[1] = {a0.z * k, a0.w * k};
+      u[2] = {a1.x * k, a1.y * k};
+      u[3] = {a1.z * k, a1.w * k};
+      u[4] = {a2.x * k, a2.y * k};
+      u[5] = {a2.z * k, a2.w * k};
       u[6] = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
       u[7] = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));
       u[8] = cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));

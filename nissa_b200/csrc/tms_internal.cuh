@@ -58,6 +58,7 @@ struct tms_ctx
   double2* U64 = nullptr;
   float4* U32r = nullptr; // 12-real
   float2* U32f = nullptr; // 18-real
+  short4* U16r = nullptr; // 12-real, 16-bit fixed point
 
   // scalars and reduction scratch
   OpParams* prm = nullptr;       // [2]: operator params (slot 0 solver, slot 1 free use)
@@ -99,6 +100,16 @@ struct tms_ctx
   cudaGraphExec_t graph[kGraphs] = {};
   int graph_iters = 8;
   uint64_t graph_nodes[kGraphs] = {};
+
+  // tuning (tms_set_tuning): hopping-kernel launch shape per precision, the
+  // reliable-update trigger of the mixed solvers
+  int hop_cfg[3] = {0, 1, 0};
+  double delta_single = 1e-3, delta_half = 0.005;
+  int mrhs_r = 4; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
+
+  // batched-solver workspace (owned by tms_batch.cu)
+  void* bw = nullptr;
+  void (*bw_free)(void*) = nullptr;
 
   // kernels launched by this context (graph replays count their nodes)
   uint64_t launches = 0;
@@ -186,19 +197,40 @@ namespace tms_int
 
   // ------------------------------------------------------------ hop launch
   template <int P, int LF, class Epi, class Fin = NoFin>
+  void launch_hop_v(tms_ctx* c, cudaStream_t s, int par_out, int npar, const SpinorT<P>& in_e,
+                    const SpinorT<P>& in_o, const LinkT<LF>& U, const OpParams* prm, const Epi& epi,
+                    const Fin& fin = Fin{}, const int* stop = nullptr)
+  {
+    const int nsite = (int)(npar * c->g.Vh);
+    ++c->launches;
+    switch (c->hop_cfg[P])
+      {
+      case 1:
+        hop_kernel<P, LF, Epi, Fin, 1><<<div_up(nsite, HopCfg<P, 1>::NT), HopCfg<P, 1>::NT, 0, s>>>(
+          c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+        break;
+      case 2:
+        hop_kernel<P, LF, Epi, Fin, 2><<<div_up(nsite, HopCfg<P, 2>::NT), HopCfg<P, 2>::NT, 0, s>>>(
+          c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+        break;
+      default:
+        hop_kernel<P, LF, Epi, Fin, 0><<<div_up(nsite, HopCfg<P, 0>::NT), HopCfg<P, 0>::NT, 0, s>>>(
+          c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+      }
+  }
+
+  template <int P, int LF, class Epi, class Fin = NoFin>
   void launch_hop(tms_ctx* c, cudaStream_t s, int par_out, int npar, const Field& in_e, const Field& in_o,
                   const LinkT<LF>& U, const OpParams* prm, const Epi& epi, const Fin& fin = Fin{},
                   const int* stop = nullptr)
   {
-    const int nsite = (int)(npar * c->g.Vh);
-    ++c->launches;
-    hop_kernel<P, LF, Epi, Fin><<<div_up(nsite, HOP_THREADS), HOP_THREADS, 0, s>>>(
-      c->g, par_out, npar, view<P>(in_e), view<P>(in_o), U, prm, epi, reducer(c), fin, stop);
+    launch_hop_v<P, LF>(c, s, par_out, npar, view<P>(in_e), view<P>(in_o), U, prm, epi, fin, stop);
   }
 
   inline LinkT<LINK_F64_18> links64(tms_ctx* c) { return LinkT<LINK_F64_18>{c->U64, (int)c->g.Vh}; }
   inline LinkT<LINK_F32_12> links32r(tms_ctx* c) { return LinkT<LINK_F32_12>{c->U32r, (int)c->g.Vh}; }
   inline LinkT<LINK_F32_18> links32f(tms_ctx* c) { return LinkT<LINK_F32_18>{c->U32f, (int)c->g.Vh}; }
+  inline LinkT<LINK_I16_12> links16r(tms_ctx* c) { return LinkT<LINK_I16_12>{c->U16r, (int)c->g.Vh}; }
 
   // --------------------------------------------------------- conf kernels
   static __global__ void conf_to_soa_kernel(Lattice g, const double* __restrict__ src, int layout, int unfold,
@@ -224,7 +256,8 @@ namespace tms_int
 
   // FP32 copies and the special-unitarity check (max deviation over links)
   static __global__ void conf_lowprec_kernel(int64_t nlinks_per_parmu, int Vh, const double2* __restrict__ U,
-                                      float4* __restrict__ Ur, float2* __restrict__ Uf, Reducer red)
+                                      float4* __restrict__ Ur, float2* __restrict__ Uf, short4* __restrict__ Us,
+                                      Reducer red)
   {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; // over 8*Vh (par,mu,site)
     double dev = 0.0;
@@ -241,6 +274,10 @@ namespace tms_int
         Ur[((size_t)pm * 3 + 0) * Vh + site] = make_float4((float)u[0].re, (float)u[0].im, (float)u[1].re, (float)u[1].im);
         Ur[((size_t)pm * 3 + 1) * Vh + site] = make_float4((float)u[2].re, (float)u[2].im, (float)u[3].re, (float)u[3].im);
         Ur[((size_t)pm * 3 + 2) * Vh + site] = make_float4((float)u[4].re, (float)u[4].im, (float)u[5].re, (float)u[5].im);
+        auto q = [](double x) { return (short)__double2int_rn(fmin(1.0, fmax(-1.0, x)) * 32767.0); };
+        Us[((size_t)pm * 3 + 0) * Vh + site] = make_short4(q(u[0].re), q(u[0].im), q(u[1].re), q(u[1].im));
+        Us[((size_t)pm * 3 + 1) * Vh + site] = make_short4(q(u[2].re), q(u[2].im), q(u[3].re), q(u[3].im));
+        Us[((size_t)pm * 3 + 2) * Vh + site] = make_short4(q(u[4].re), q(u[4].im), q(u[5].re), q(u[5].im));
         // deviation of row 2 from conj(row0 x row1), plus row-0/1 unitarity
         const C<double> c0 = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
         const C<double> c1 = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));
@@ -409,17 +446,6 @@ namespace tms_int
     s.d += off;
     if (s.n) s.n += off;
     return s;
-  }
-
-  template <int P, int LF, class Epi, class Fin = NoFin>
-  void launch_hop_v(tms_ctx* c, cudaStream_t s, int par_out, int npar, const SpinorT<P>& in_e,
-                    const SpinorT<P>& in_o, const LinkT<LF>& U, const OpParams* prm, const Epi& epi,
-                    const Fin& fin = Fin{}, const int* stop = nullptr)
-  {
-    const int nsite = (int)(npar * c->g.Vh);
-    ++c->launches;
-    hop_kernel<P, LF, Epi, Fin><<<div_up(nsite, HOP_THREADS), HOP_THREADS, 0, s>>>(c->g, par_out, npar, in_e, in_o,
-                                                                                  U, prm, epi, reducer(c), fin, stop);
   }
 
   // lx AoS spinor (V rows of 24 doubles, host or device) <-> full-lattice FP64 field

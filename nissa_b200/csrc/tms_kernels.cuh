@@ -701,14 +701,27 @@ namespace tms
   // ---------------------------------------------------------- hop kernel
   // Launch: one thread per output site; npar = 1 computes the parity
   // par_out only, npar = 2 both parities (grid over 2*Vh).
-  template <int P, int LF, class Epi, class Fin>
-  __global__ void __launch_bounds__(HOP_THREADS)
+  // Launch shapes the autotuner chooses from (per precision):
+  //   CFG 0: 128 threads, no register cap
+  //   CFG 1: 128 threads, registers capped for 4 (FP64) / 8 (FP32, FP16) resident blocks per SM
+  //   CFG 2: 256 threads, registers capped for 2 (FP64) / 4 (FP32, FP16) resident blocks per SM
+  template <int P, int CFG>
+  struct HopCfg
+  {
+    static constexpr int NT = (CFG == 2) ? 256 : 128;
+    static constexpr int MINB = (CFG == 0) ? 1 : (CFG == 1) ? (P == PREC_F64 ? 4 : 8) : (P == PREC_F64 ? 2 : 4);
+  };
+  constexpr int HOP_CFGS = 3;
+
+  template <int P, int LF, class Epi, class Fin, int CFG = 0>
+  __global__ void __launch_bounds__(HopCfg<P, CFG>::NT, HopCfg<P, CFG>::MINB)
     hop_kernel(Lattice g, int par_out, int npar, SpinorT<P> in_e, SpinorT<P> in_o, LinkT<LF> U, const OpParams* prm,
                Epi epi, Reducer red, Fin fin, const int* __restrict__ stop)
   {
     using R = typename SpinorT<P>::R;
+    constexpr int NT = HopCfg<P, CFG>::NT;
     if (stop && *stop) return;
-    const int idx = blockIdx.x * HOP_THREADS + threadIdx.x;
+    const int idx = blockIdx.x * NT + threadIdx.x;
     int p = par_out, ieo = idx;
     if (npar == 2)
       {
@@ -724,7 +737,7 @@ namespace tms
         hop_site<P, LF>(g, p, ieo, p ? in_e : in_o, U, anis, acc);
         part = epi(p, ieo, acc);
       }
-    if (Epi::kReduce) grid_reduce<HOP_THREADS>(part, red, fin);
+    if (Epi::kReduce) grid_reduce<NT>(part, red, fin);
   }
 
   // ------------------------------------------------------- BLAS kernels

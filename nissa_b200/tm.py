@@ -201,12 +201,24 @@ class Lattice:
         """CUDA kernels launched by this lattice's context so far."""
         return int(self.lib.tms_launch_count(self.h))
 
+    def set_tuning(self, key: str, value: float):
+        """Set a tuning knob of the C ABI (see tms_set_tuning in include/tmsolve.h)."""
+        self._check(self.lib.tms_set_tuning(self.h, key.encode(), float(value)), "tms_set_tuning")
+
     def bench_hop(self, precision="double", variant=0, nrep=20, flush=True):
         """Mean device time (ms) of one e/o hopping launch and its algorithmic bytes."""
         ms, by = ctypes.c_double(), ctypes.c_double()
         st = self.lib.tms_bench_hop(self.h, PRECISION[precision], int(variant), int(nrep), 1 if flush else 0,
                                     ctypes.byref(ms), ctypes.byref(by))
         self._check(st, "tms_bench_hop")
+        return ms.value, by.value
+
+    def bench_hop_batched(self, precision="single", nrhs=12, nrep=20, flush=True):
+        """Mean device time (ms) of one batched hopping launch and its algorithmic bytes."""
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        st = self.lib.tms_bench_hop_batched(self.h, PRECISION[precision], int(nrhs), int(nrep), 1 if flush else 0,
+                                            ctypes.byref(ms), ctypes.byref(by))
+        self._check(st, "tms_bench_hop_batched")
         return ms.value, by.value
 
     # ------------------------------------------------------------ solvers
@@ -263,6 +275,32 @@ class Lattice:
         sd = [x.as_dict() for x in stats]
         if raise_on_error:
             self._check(st, "inv_tmQ2_cgm", sd, out)
+        return out, sd
+
+    def inv_tmD_cg_eoprec_batched(self, kappa, mus, sources_lx, niter, residues, anis=None, precision="double",
+                                  out=None, raise_on_error=True):
+        """inv_tmD_cg_eoprec for several sources (one twisted mass each) solved
+        together.  Returns (sols, [stats])."""
+        shape = (self.V, 4, 3, 2)
+        nr = len(sources_lx)
+        mus = np.broadcast_to(np.asarray(mus, np.float64), (nr,)).copy()
+        residues = np.broadcast_to(np.asarray(residues, np.float64), (nr,)).copy()
+        sb = [_Buf(x, shape) for x in sources_lx]
+        if out is None:
+            out = [self._new_out(sources_lx[0], shape) for _ in range(nr)]
+        ob = [_Buf(o, shape, out=True) for o in out]
+        self._mode(*sb, *ob)
+        sp = (ctypes.c_void_p * nr)(*[b.ptr for b in sb])
+        op = (ctypes.c_void_p * nr)(*[b.ptr for b in ob])
+        stats = (_lib.Stats * nr)()
+        a = self._anis(anis)
+        st = self.lib.tms_cg_eoprec_batched(self.h, nr, ctypes.cast(op, ctypes.c_void_p),
+                                            ctypes.cast(sp, ctypes.c_void_p), kappa, a[0], a[1], mus.ctypes.data,
+                                            int(niter), residues.ctypes.data, PRECISION[precision],
+                                            ctypes.cast(stats, ctypes.c_void_p))
+        sd = [x.as_dict() for x in stats]
+        if raise_on_error:
+            self._check(st, "inv_tmD_cg_eoprec_batched", sd, out)
         return out, sd
 
     def inv_tmD_cg_eoprec(self, kappa, mu, source_lx, niter, residue, anis=None, precision="double", out=None,

@@ -121,3 +121,19 @@ def test_precision_switching_same_lattice(cuda_device):
         n0 = lat.launch_count
         lat.inv_tmDkern_eoprec_square_eos_cg(0.16, 0.01, src, 10000, 1e-20, precision="single")
         assert lat.launch_count - n0 >= 5 * 10
+
+
+@pytest.mark.parametrize("precision", ["double", "single", "half"])
+def test_full_solve_point_source_all_precisions(cuda_device, golden_cg, precision):
+    """The 8^3x16 point-source solve in every precision: a point source leaves
+    most sites at (or near) zero for many iterations, which the FP16 per-site
+    scale must survive."""
+    g = golden_cg
+    T, L = int(g["T"]), int(g["L"])
+    conf = wl.gauge_conf(T, L, float(g["eps"]), int(g["seed"]))
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        sol, st = lat.inv_tmD_cg_eoprec(float(g["kappa"]), float(g["mu"]), wl.point_source(T, L), 100000, 1e-24,
+                                        precision=precision)
+        assert st["true_rel_res2"] < 1e-24
+        assert rel(sol[::8], g["sol_every8"]) < 1e-9
