@@ -384,6 +384,37 @@ def run_cgm(args):
           flush=True)
 
 
+SERVE_WORKLOAD = dict(volumes={"8^3x16": (16, 8), "16^3x32": (32, 16), "32^3x64": (64, 32)},
+                      probs=[0.5, 0.35, 0.15], eps=0.35, seed=1, rate=20.0, requests=200, nslots=16)
+
+
+def run_serve(args):
+    """The serving workload: three resident configurations, Poisson arrivals
+    at a stated rate, requests batched continuously per volume; prints p50/p99
+    latency and throughput (an extra report, not the headline)."""
+    from nissa_b200 import workload as wl
+    from nissa_b200.serve import GpuResidency, SolveServer, latency_summary, poisson_requests, run_load
+    W = SERVE_WORKLOAD
+    rate = args.rate or W["rate"]
+    n = args.requests or W["requests"]
+    vols = {k: (T, L, wl.gauge_conf(T, L, W["eps"], W["seed"], device="cuda:0")) for k, (T, L) in W["volumes"].items()}
+    res = GpuResidency(vols, nslots=W["nslots"], precision=args.serve_precision)
+    srv = SolveServer(res.backends(), free_memory=res.free_memory, reserve_bytes=2 << 30)
+    warm = poisson_requests(6, rate=100.0, volumes=list(vols), probs=[1 / 3] * 3, seed=99)
+    run_load(srv, warm)
+    sched = poisson_requests(n, rate=rate, volumes=list(vols), probs=W["probs"], seed=W["seed"])
+    with ClockSampler(0) as clk:
+        results, wall = run_load(srv, sched)
+    srv.close()
+    summ = latency_summary(results, wall)
+    summ.update({"workload": "serving: resident 8^3x16, 16^3x32, 32^3x64; Poisson arrivals",
+                 "rate_per_s": rate, "precision": args.serve_precision, "slots_per_volume": W["nslots"],
+                 "max_true_rel_res2_over_target": max(r.stats["true_rel_res2"] / r.request.residue for r in results),
+                 "failed": sum(r.stats["status"] != 0 for r in results), "clocks": clk.summary()})
+    res.close()
+    print(json.dumps(summ), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -400,8 +431,11 @@ def main():
     ap.add_argument("--nrep", type=int, default=10, help="launches for --kernel-only")
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
-    ap.add_argument("--workload", default="cg", choices=["cg", "cgm"],
-                    help="cg: the headline solve; cgm: the multi-shift workload (extra report)")
+    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve"],
+                    help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop (extra reports)")
+    ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--requests", type=int, default=0, help="serve: number of requests")
+    ap.add_argument("--serve-precision", default="single", choices=["double", "single", "half"])
     ap.add_argument("--cgm-precision", default="single", choices=["single", "half"])
     args = ap.parse_args()
     if args.lattice:
@@ -412,6 +446,9 @@ def main():
         return
     if args.workload == "cgm":
         run_cgm(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)

@@ -159,6 +159,23 @@ tms_status tms_cg_eoprec_batched(tms_ctx *ctx, int nrhs, double *const *sols_lx,
                                  double kappa, int has_anis, double anis, const double *mus, int niter,
                                  const double *residues, int precision, tms_stats *stats);
 
+/* ---- batch sessions (continuous batching; no reference counterpart) ----
+ * A session keeps up to nslots (<= 64) solves of inv_tmD_cg_eoprec in flight on one context, each
+ * with its own kappa, mu and residue: submit puts a right-hand side into a free slot (the source is
+ * prepared at once, Eq. 8), step runs one CUDA-graph block of lock-step CG iterations for all
+ * running slots and reports the slots that finished, collect writes a finished slot's solution
+ * (Eq. 10-11) and frees the slot.  New right-hand sides can be submitted between steps while
+ * others are still iterating.  One session per context at a time; one host thread per context. */
+typedef struct tms_batch tms_batch;
+tms_status tms_batch_open(tms_ctx *ctx, int nslots, int precision, int has_anis, double anis, tms_batch **batch);
+tms_status tms_batch_submit(tms_batch *batch, int slot, const double *src_lx, double kappa, double mu, int niter,
+                            double residue);
+/* finished[nslots] (out): 1 for the slots that finished in this step; *nfinished (may be NULL) their count */
+tms_status tms_batch_step(tms_batch *batch, int *finished, int *nfinished);
+/* returns the solve's status (TMS_OK, TMS_ERR_NOT_CONVERGED, TMS_ERR_NAN) */
+tms_status tms_batch_collect(tms_batch *batch, int slot, double *sol_lx, tms_stats *stats);
+tms_status tms_batch_close(tms_batch *batch);
+
 /* ---- instrumentation (no reference counterpart) ---- */
 
 /* Number of CUDA kernels this context has launched (CUDA-graph replays count their nodes). */

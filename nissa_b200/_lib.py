@@ -45,6 +45,11 @@ SIGNATURES = {
     "tms_cg_tmQ2": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cgm_tmQ2": (I, [P, P, P, D, I, D, P, I, I, P, I, P]),
     "tms_cg_eoprec_batched": (I, [P, I, P, P, D, I, D, P, I, P, I, P]),
+    "tms_batch_open": (I, [P, I, I, I, D, ctypes.POINTER(P)]),
+    "tms_batch_submit": (I, [P, I, P, D, D, I, D]),
+    "tms_batch_step": (I, [P, P, ctypes.POINTER(I)]),
+    "tms_batch_collect": (I, [P, I, P, ctypes.POINTER(Stats)]),
+    "tms_batch_close": (I, [P]),
     "tms_launch_count": (ctypes.c_uint64, [P]),
     "tms_set_tuning": (I, [P, ctypes.c_char_p, D]),
     "tms_bench_hop": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),

@@ -1,10 +1,12 @@
-// Batched e/o solves: k right-hand sides with one kappa and a twisted mass
-// each, solved together so that every hop of the CG reads the links once for
-// all of them (the reference solves them one inv_tmD_cg_eoprec call at a time).
+// Batched e/o solves: k right-hand sides, each with its own kappa and twisted
+// mass, solved together so that every hop of the CG reads the links once for
+// all of them (the reference solves them one inv_tmD_cg_eoprec call at a time),
+// and batch sessions that admit new right-hand sides as others finish.
 #include "tms_internal.cuh"
 #include "tms_batch.cuh"
 
 #include <algorithm>
+#include <chrono>
 
 using namespace tms_int;
 
@@ -60,6 +62,7 @@ namespace
     cudaGraphExec_t graph[3] = {};
     uint64_t nodes[3] = {};
     int graph_nrhs[3] = {};
+    bool open = false;    // a batch session owns the buffers
   };
 
   void free_bfield(BField& f)
@@ -184,305 +187,9 @@ namespace
     return TMS_OK;
   }
 
-  tms_status push_mask(tms_ctx* ctx, BatchWork* w, int nrhs)
-  {
-    CU(cudaMemcpyAsync(w->mask, w->mask_h, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
-    return TMS_OK;
-  }
 
-  // Lock-step CG on K(+mu_k)K(-mu_k) for nrhs odd sources hi[0], solutions in
-  // hi[1].  Inner precision P (FP64: plain CG as in cg_invert; FP32/FP16: FP64
-  // reliable updates of the right-hand sides that ask for one).
-  template <int P, int LF>
-  tms_status cg_batch(tms_ctx* ctx, BatchWork* w, const LinkT<LF>& U, int nrhs, int niter, const double* residue,
-                      tms_stats* stats)
-  {
-    constexpr int PX = (P == PREC_F16) ? PREC_F32 : P;
-    const int slot = P;
-    const int n = (int)ctx->g.Vh;
-    const bool mixed = (P != PREC_F64);
-    for (int i = 1; i <= 5; i++) TRY(alloc_bfield(ctx, w->hi[i], PREC_F64, nrhs));
-    if (w->lo_prec != P || w->lo[1].nrhs < nrhs)
-      for (auto& g : w->graph)
-        if (g)
-          {
-            CU(cudaStreamSynchronize(ctx->stream));
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-          }
-    for (int i = 1; i <= 4; i++) TRY(alloc_bfield(ctx, w->lo[i], P, nrhs));
-    TRY(alloc_bfield(ctx, w->xlo, PX, nrhs));
-    w->lo_prec = P;
-    const double delta = (P == PREC_F16) ? ctx->delta_half : ctx->delta_single;
-    const dim3 bg(blas_grid(ctx), nrhs);
 
-    // |b_k|^2: the residual of x = 0 against b
-    CU(cudaMemsetAsync(w->hi[1].d, 0, w->hi[1].bytes, ctx->stream));
-    for (int k = 0; k < nrhs; k++) w->mask_h[k].stop = 0;
-    TRY(push_mask(ctx, w, nrhs));
-    std::vector<double> b2(nrhs), rr(nrhs);
-    TRY(true_residual_b(ctx, w, nrhs, w->hi[1], b2.data()));
-    for (int k = 0; k < nrhs; k++)
-      if (b2[k] == 0.0 || std::isnan(b2[k]))
-        return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm of right-hand side %d: %g", k, b2[k]);
-    // r = b (in hi[2] already), r_lo = r, p_lo = r, x_lo = 0
-    ++ctx->launches;
-    axpby_mrhs_kernel<P, PREC_F64, PREC_F64><<<bg, 256, 0, ctx->stream>>>(
-      n, nrhs, 1.0, bview<PREC_F64>(w->hi[2]), 0.0, bview<PREC_F64>(w->hi[2]), bview<P>(w->lo[1]), nullptr);
-    ++ctx->launches;
-    axpby_mrhs_kernel<P, PREC_F64, PREC_F64><<<bg, 256, 0, ctx->stream>>>(
-      n, nrhs, 1.0, bview<PREC_F64>(w->hi[2]), 0.0, bview<PREC_F64>(w->hi[2]), bview<P>(w->lo[2]), nullptr);
-    CU(cudaMemsetAsync(w->xlo.d, 0, w->xlo.bytes, ctx->stream));
-    std::vector<int> done(nrhs, 0), reliable(nrhs, 0);
-    std::vector<double> tres(nrhs, 0.0);
-    std::vector<tms_status> status(nrhs, TMS_OK);
-    CgState* S = w->st_h;
-    for (int k = 0; k < nrhs; k++)
-      {
-        memset(&S[k], 0, sizeof(CgState));
-        S[k].rr = b2[k];
-        S[k].b2 = b2[k];
-        S[k].target = residue[k] * b2[k];
-        S[k].rel_trigger = mixed ? delta * delta * b2[k] : -1.0;
-        S[k].niter_max = niter;
-      }
-    CU(cudaMemcpyAsync(w->st, S, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
-    // graph of graph_iters lock-step iterations for this nrhs
-    if (w->graph[slot] && w->graph_nrhs[slot] != nrhs)
-      {
-        CU(cudaStreamSynchronize(ctx->stream));
-        cudaGraphExecDestroy(w->graph[slot]);
-        w->graph[slot] = nullptr;
-      }
-    if (!w->graph[slot])
-      {
-        cudaStream_t cs;
-        CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        cudaGraph_t graph;
-        CU(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        const uint64_t before = ctx->launches;
-        for (int it = 0; it < ctx->graph_iters; it++)
-          {
-            EpiBInvDiag<P> a1{bview<P>(w->lo[4]), -1.0};
-            launch_mrhs<P>(ctx, w, cs, 0, nrhs, w->lo[2], U, a1, NoFinB{}, w->st);
-            EpiBKern<P, true> b1{bview<P>(w->lo[3]), bview<P>(w->lo[2]), -1.0};
-            launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b1, FinAlphaB{w->st}, w->st);
-            EpiBInvDiag<P> a2{bview<P>(w->lo[4]), +1.0};
-            launch_mrhs<P>(ctx, w, cs, 0, nrhs, w->lo[3], U, a2, NoFinB{}, w->st);
-            EpiBKernCgUpdate<P, PX> b2e{bview<P>(w->lo[3]), bview<P>(w->lo[1]), bview<P>(w->lo[2]), bview<PX>(w->xlo),
-                                        w->st, +1.0};
-            launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b2e, FinBetaB{w->st}, w->st);
-            ++ctx->launches;
-            xpay_mrhs_kernel<P><<<bg, 256, 0, cs>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]), w->st, nullptr);
-          }
-        w->nodes[slot] = ctx->launches - before;
-        ctx->launches = before;
-        cudaError_t e = cudaStreamEndCapture(cs, &graph);
-        cudaStreamDestroy(cs);
-        if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&w->graph[slot], graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-        w->graph_nrhs[slot] = nrhs;
-      }
-    CU(cudaEventRecord(ctx->ev0, ctx->stream));
-    int ndone = 0;
-    while (ndone < nrhs)
-      {
-        CU(cudaGraphLaunch(w->graph[slot], ctx->stream));
-        ctx->launches += w->nodes[slot];
-        CU(cudaMemcpyAsync(S, w->st, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
-        // right-hand sides that stopped: finish them, or update and restart them
-        bool any = false;
-        for (int k = 0; k < nrhs; k++)
-          {
-            w->mask_h[k].stop = 1;
-            if (done[k] || S[k].stop == STOP_RUN) continue;
-            if (S[k].stop == STOP_BREAKDOWN)
-              {
-                status[k] = TMS_ERR_NAN;
-                done[k] = 1;
-                ndone++;
-                continue;
-              }
-            if (!mixed)
-              {
-                status[k] = (S[k].stop == STOP_MAXITER) ? TMS_ERR_NOT_CONVERGED : TMS_OK;
-                done[k] = 1;
-                ndone++;
-                continue;
-              }
-            w->mask_h[k].stop = 0; // take part in the reliable update
-            any = true;
-          }
-        if (!mixed)
-          {
-            // keep the finished ones out of the graph's kernels
-            continue;
-          }
-        if (!any) continue;
-        TRY(push_mask(ctx, w, nrhs));
-        // x += x_lo ; x_lo = 0 (for the masked right-hand sides)
-        ++ctx->launches;
-        axpby_mrhs_kernel<PREC_F64, PREC_F64, PX><<<bg, 256, 0, ctx->stream>>>(
-          n, nrhs, 1.0, bview<PREC_F64>(w->hi[1]), 1.0, bview<PX>(w->xlo), bview<PREC_F64>(w->hi[1]), w->mask);
-        ++ctx->launches;
-        axpby_mrhs_kernel<PX, PX, PX><<<bg, 256, 0, ctx->stream>>>(n, nrhs, 0.0, bview<PX>(w->xlo), 0.0,
-                                                                   bview<PX>(w->xlo), bview<PX>(w->xlo), w->mask);
-        TRY(true_residual_b(ctx, w, nrhs, w->hi[1], rr.data()));
-        bool restart = false;
-        for (int k = 0; k < nrhs; k++)
-          {
-            if (w->mask_h[k].stop) continue;
-            reliable[k]++;
-            tres[k] = rr[k];
-            if (rr[k] < S[k].target || S[k].stop == STOP_MAXITER || S[k].iter >= niter)
-              {
-                status[k] = (rr[k] < S[k].target) ? TMS_OK : TMS_ERR_NOT_CONVERGED;
-                done[k] = 1;
-                ndone++;
-                S[k].stop = 5; // finished: the graph's kernels skip it
-                w->mask_h[k].stop = 1;
-                continue;
-              }
-            S[k].beta = rr[k] / S[k].rr_prev;
-            S[k].rr = rr[k];
-            S[k].rel_trigger = delta * delta * rr[k];
-            S[k].stop = STOP_RUN;
-            restart = true;
-          }
-        if (restart)
-          {
-            TRY(push_mask(ctx, w, nrhs));
-            // r_lo = r ; p_lo = r_lo + beta p_lo  (masked)
-            ++ctx->launches;
-            axpby_mrhs_kernel<P, PREC_F64, PREC_F64><<<bg, 256, 0, ctx->stream>>>(
-              n, nrhs, 1.0, bview<PREC_F64>(w->hi[2]), 0.0, bview<PREC_F64>(w->hi[2]), bview<P>(w->lo[1]), w->mask);
-          }
-        CU(cudaMemcpyAsync(w->st, S, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
-        if (restart)
-          {
-            ++ctx->launches;
-            xpay_mrhs_kernel<P><<<bg, 256, 0, ctx->stream>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]), w->st,
-                                                             w->mask);
-          }
-        CU(cudaGetLastError());
-      }
-    CU(cudaEventRecord(ctx->ev1, ctx->stream));
-    CU(cudaEventSynchronize(ctx->ev1));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    if (!mixed)
-      {
-        // the FP64 iteration accumulated x in the inner field
-        ++ctx->launches;
-        axpby_mrhs_kernel<PREC_F64, PX, PX><<<bg, 256, 0, ctx->stream>>>(n, nrhs, 1.0, bview<PX>(w->xlo), 0.0,
-                                                                         bview<PX>(w->xlo), bview<PREC_F64>(w->hi[1]),
-                                                                         nullptr);
-        for (int k = 0; k < nrhs; k++) w->mask_h[k].stop = 0;
-        TRY(push_mask(ctx, w, nrhs));
-        TRY(true_residual_b(ctx, w, nrhs, w->hi[1], tres.data()));
-      }
-    tms_status worst = TMS_OK;
-    for (int k = 0; k < nrhs; k++)
-      {
-        if (stats)
-          {
-            stats[k].status = status[k];
-            stats[k].iterations = S[k].iter;
-            stats[k].reliable_updates = reliable[k];
-            stats[k].iterated_rel_res2 = S[k].rr / b2[k];
-            stats[k].true_rel_res2 = tres[k] / b2[k];
-            stats[k].seconds = ms * 1e-3;
-          }
-        if (status[k] != TMS_OK && worst == TMS_OK) worst = status[k];
-      }
-    if (worst == TMS_ERR_NAN) return fail(ctx, worst, "nanned");
-    if (worst == TMS_ERR_NOT_CONVERGED) return fail(ctx, worst, "exit without converging");
-    return TMS_OK;
-  }
-}
 
-extern "C" tms_status tms_cg_eoprec_batched(tms_ctx* ctx, int nrhs, double* const* sols_lx,
-                                             const double* const* srcs_lx, double kappa, int has_anis, double anis,
-                                             const double* mus, int niter, const double* residues, int precision,
-                                             tms_stats* stats)
-{
-  TRY(check_conf(ctx));
-  if (nrhs <= 0 || nrhs > MRHS_MAX || !sols_lx || !srcs_lx || !mus || !residues || niter <= 0)
-    return fail(ctx, TMS_ERR_BAD_ARG, "bad batched arguments (1 <= nrhs <= %d)", MRHS_MAX);
-  for (int k = 0; k < nrhs; k++)
-    if (!sols_lx[k] || !srcs_lx[k] || !(residues[k] > 0) || !std::isfinite(mus[k]))
-      return fail(ctx, TMS_ERR_BAD_ARG, "bad right-hand side %d", k);
-  if (precision != TMS_PREC_DOUBLE && precision != TMS_PREC_MIXED_SINGLE && precision != TMS_PREC_MIXED_HALF)
-    return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
-  BatchWork* w;
-  TRY(work(ctx, &w));
-  TRY(alloc_bfield(ctx, w->hi[0], PREC_F64, nrhs));
-  TRY(alloc_bfield(ctx, w->hi[6], PREC_F64, nrhs)); // eta_e per right-hand side
-  Field* f = ctx->f64;
-  for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
-  Field *eta = ctx->ex, *psi = ctx->ex + 2;
-  for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
-  BatchParams& bp = *w->bp_h;
-  bp.kappa = kappa;
-  bp.anis = has_anis ? anis : 1.0;
-  for (int k = 0; k < nrhs; k++) bp.mu[k] = mus[k];
-  CU(cudaMemcpyAsync(w->bp, w->bp_h, sizeof(BatchParams), cudaMemcpyHostToDevice, ctx->stream));
-  const int64_t Vh = ctx->g.Vh;
-  const int n = (int)Vh;
-  const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
-  auto U = links64(ctx);
-  auto V = [](const Field& x) { return view<PREC_F64>(x); };
-  // Eq. (8) per right-hand side (single-RHS FP64 kernels): varphi_k -> hi[0][k], eta_e,k -> hi[6][k]
-  for (int k = 0; k < nrhs; k++)
-    {
-      TRY(set_params(ctx, kappa, mus[k], has_anis, anis));
-      const double* src = srcs_lx[k];
-      if (ctx->ptr_mode == TMS_PTR_HOST)
-        {
-          TRY(ensure_stage(ctx, bytes));
-          CU(cudaMemcpyAsync(ctx->stage, srcs_lx[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
-          src = ctx->stage;
-        }
-      const Field ek = one(w->hi[6], k), vk = one(w->hi[0], k);
-      ctx->launches += 4;
-      aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(ek));
-      aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
-      diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(ek), V(f[5]), ctx->prm, 1.0, 1);
-      EpiSrcPrep<PREC_F64> sp{{V(vk), V(vk)}, {V(eta[1]), V(eta[1])}};
-      launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
-      CU(cudaGetLastError());
-    }
-  // Eq. (9), all right-hand sides at once
-  tms_status st;
-  if (precision == TMS_PREC_DOUBLE) st = cg_batch<PREC_F64>(ctx, w, links64(ctx), nrhs, niter, residues, stats);
-  else if (precision == TMS_PREC_MIXED_SINGLE)
-    st = ctx->su3 ? cg_batch<PREC_F32>(ctx, w, links32r(ctx), nrhs, niter, residues, stats)
-                  : cg_batch<PREC_F32>(ctx, w, links32f(ctx), nrhs, niter, residues, stats);
-  else
-    st = ctx->su3 ? cg_batch<PREC_F16>(ctx, w, links16r(ctx), nrhs, niter, residues, stats)
-                  : cg_batch<PREC_F16>(ctx, w, links32f(ctx), nrhs, niter, residues, stats);
-  if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
-  // Eq. (10)-(11) and paste, per right-hand side
-  for (int k = 0; k < nrhs; k++)
-    {
-      TRY(set_params(ctx, kappa, mus[k], has_anis, anis));
-      const Field xk = one(w->hi[1], k), ek = one(w->hi[6], k);
-      kern_op<PREC_F64>(ctx, U, xk, f[5], psi[1], -1.0, ctx->prm);
-      EpiReco<PREC_F64> rc{{V(psi[0]), V(psi[0])}, {V(ek), V(ek)}, ctx->prm, 1.0};
-      launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
-      double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sols_lx[k];
-      ctx->launches += 2;
-      soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, d);
-      soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, d);
-      CU(cudaGetLastError());
-      if (ctx->ptr_mode == TMS_PTR_HOST)
-        CU(cudaMemcpyAsync(sols_lx[k], ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    }
-  TRY(finish(ctx));
-  return st;
 }
 
 namespace
@@ -494,9 +201,12 @@ namespace
     TRY(alloc_bfield(ctx, w->lo[1], P, nrhs));
     TRY(alloc_bfield(ctx, w->lo[2], P, nrhs));
     BatchParams& bp = *w->bp_h;
-    bp.kappa = 0.16;
     bp.anis = 1.0;
-    for (int k = 0; k < nrhs; k++) bp.mu[k] = 0.01;
+    for (int k = 0; k < nrhs; k++)
+      {
+        bp.kappa[k] = 0.16;
+        bp.mu[k] = 0.01;
+      }
     CU(cudaMemcpyAsync(w->bp, w->bp_h, sizeof(BatchParams), cudaMemcpyHostToDevice, ctx->stream));
     void* scratch = nullptr;
     const size_t sbytes = size_t(512) << 20;
@@ -550,3 +260,477 @@ extern "C" tms_status tms_bench_hop_batched(tms_ctx* ctx, int precision, int nrh
                                              bytes_per_launch);
   return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
 }
+
+// ===================================================== batch sessions
+// A session keeps nslots right-hand sides of one lattice in flight: a
+// right-hand side is submitted into a free slot (its source prepared by
+// Eq. 8), every step runs one CUDA-graph block of lock-step CG iterations
+// for all running slots (and the FP64 reliable updates of the slots that ask
+// for one), and a converged slot is collected (Eq. 10-11) and freed for the
+// next right-hand side while the others keep iterating.
+
+constexpr int SLOT_FREE = 0, SLOT_RUNNING = 1, SLOT_FINISHED = 2;
+constexpr int STOP_IDLE = 5; // CgState.stop of a slot that is not iterating
+
+struct tms_batch
+{
+  tms_ctx* ctx = nullptr;
+  BatchWork* w = nullptr;
+  int nslots = 0, prec = 0, has_anis = 0;
+  double anis = 1.0;
+  std::vector<int> state;
+  std::vector<double> b2, tres;
+  std::vector<int> reliable, niter;
+  std::vector<tms_status> status;
+  std::vector<std::chrono::steady_clock::time_point> t0;
+  std::vector<double> secs;
+};
+
+namespace
+{
+  tms_status open_fields(tms_batch* b)
+  {
+    tms_ctx* ctx = b->ctx;
+    BatchWork* w = b->w;
+    const int n = b->nslots;
+    for (int i = 0; i <= 6; i++) TRY(alloc_bfield(ctx, w->hi[i], PREC_F64, n));
+    const int P = b->prec == TMS_PREC_DOUBLE ? PREC_F64 : b->prec == TMS_PREC_MIXED_SINGLE ? PREC_F32 : PREC_F16;
+    const int PX = (P == PREC_F16) ? PREC_F32 : P;
+    if (w->lo_prec != P || w->lo[1].nrhs < n || w->xlo.prec != PX)
+      for (auto& g : w->graph)
+        if (g)
+          {
+            CU(cudaStreamSynchronize(ctx->stream));
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+          }
+    for (int i = 1; i <= 4; i++) TRY(alloc_bfield(ctx, w->lo[i], P, n));
+    TRY(alloc_bfield(ctx, w->xlo, PX, n));
+    w->lo_prec = P;
+    return TMS_OK;
+  }
+
+  // capture graph_iters lock-step iterations over all nslots slots
+  template <int P, int LF>
+  tms_status session_graph(tms_batch* b, const LinkT<LF>& U)
+  {
+    constexpr int PX = (P == PREC_F16) ? PREC_F32 : P;
+    tms_ctx* ctx = b->ctx;
+    BatchWork* w = b->w;
+    const int slot = P, nrhs = b->nslots, n = (int)ctx->g.Vh;
+    if (w->graph[slot] && w->graph_nrhs[slot] == nrhs) return TMS_OK;
+    if (w->graph[slot])
+      {
+        CU(cudaStreamSynchronize(ctx->stream));
+        cudaGraphExecDestroy(w->graph[slot]);
+        w->graph[slot] = nullptr;
+      }
+    const dim3 bg(blas_grid(ctx), nrhs);
+    cudaStream_t cs;
+    CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph;
+    CU(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = ctx->launches;
+    for (int it = 0; it < ctx->graph_iters; it++)
+      {
+        EpiBInvDiag<P> a1{bview<P>(w->lo[4]), -1.0};
+        launch_mrhs<P>(ctx, w, cs, 0, nrhs, w->lo[2], U, a1, NoFinB{}, w->st);
+        EpiBKern<P, true> b1{bview<P>(w->lo[3]), bview<P>(w->lo[2]), -1.0};
+        launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b1, FinAlphaB{w->st}, w->st);
+        EpiBInvDiag<P> a2{bview<P>(w->lo[4]), +1.0};
+        launch_mrhs<P>(ctx, w, cs, 0, nrhs, w->lo[3], U, a2, NoFinB{}, w->st);
+        EpiBKernCgUpdate<P, PX> b2e{bview<P>(w->lo[3]), bview<P>(w->lo[1]), bview<P>(w->lo[2]), bview<PX>(w->xlo),
+                                    w->st, +1.0};
+        launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b2e, FinBetaB{w->st}, w->st);
+        ++ctx->launches;
+        xpay_mrhs_kernel<P><<<bg, 256, 0, cs>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]), w->st, nullptr);
+      }
+    w->nodes[slot] = ctx->launches - before;
+    ctx->launches = before;
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&w->graph[slot], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    w->graph_nrhs[slot] = nrhs;
+    return TMS_OK;
+  }
+
+  template <int P>
+  tms_status session_submit(tms_batch* b, int k, double residue, int niter)
+  {
+    constexpr int PX = (P == PREC_F16) ? PREC_F32 : P;
+    tms_ctx* ctx = b->ctx;
+    BatchWork* w = b->w;
+    const int n = (int)ctx->g.Vh;
+    // varphi (the CG source) is in hi[0][k]: |b|^2
+    double b2;
+    TRY(norm2<PREC_F64>(ctx, one(w->hi[0], k), &b2));
+    if (b2 == 0.0 || std::isnan(b2)) return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm: %g", b2);
+    const Field x = one(w->hi[1], k), r = one(w->hi[2], k), v = one(w->hi[0], k);
+    CU(cudaMemsetAsync(x.d, 0, x.bytes, ctx->stream));
+    CU(cudaMemcpyAsync(r.d, v.d, v.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    convert<P, PREC_F64>(ctx, v, one(w->lo[1], k));
+    convert<P, PREC_F64>(ctx, v, one(w->lo[2], k));
+    const Field xl = one(w->xlo, k);
+    CU(cudaMemsetAsync(xl.d, 0, xl.bytes, ctx->stream));
+    (void)n;
+    (void)sizeof(PX);
+    const bool mixed = (P != PREC_F64);
+    const double delta = (P == PREC_F16) ? ctx->delta_half : ctx->delta_single;
+    CgState& S = w->st_h[k];
+    memset(&S, 0, sizeof S);
+    S.rr = b2;
+    S.b2 = b2;
+    S.target = residue * b2;
+    S.rel_trigger = mixed ? delta * delta * b2 : -1.0;
+    S.niter_max = niter;
+    S.stop = STOP_RUN;
+    CU(cudaMemcpyAsync(w->st + k, &S, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(w->bp, w->bp_h, sizeof(BatchParams), cudaMemcpyHostToDevice, ctx->stream));
+    b->b2[k] = b2;
+    b->tres[k] = 0.0;
+    b->reliable[k] = 0;
+    b->niter[k] = niter;
+    b->status[k] = TMS_OK;
+    return TMS_OK;
+  }
+
+  // one graph block for all running slots, then the slots that stopped are
+  // finished (FP64) or updated in FP64 and either finished or restarted (mixed)
+  template <int P, int LF>
+  tms_status session_step(tms_batch* b, const LinkT<LF>& U, int* finished)
+  {
+    constexpr int PX = (P == PREC_F16) ? PREC_F32 : P;
+    tms_ctx* ctx = b->ctx;
+    BatchWork* w = b->w;
+    const int nrhs = b->nslots, n = (int)ctx->g.Vh, slot = P;
+    const bool mixed = (P != PREC_F64);
+    const double delta = (P == PREC_F16) ? ctx->delta_half : ctx->delta_single;
+    const dim3 bg(blas_grid(ctx), nrhs);
+    CgState* S = w->st_h;
+    TRY(session_graph<P>(b, U));
+    CU(cudaGraphLaunch(w->graph[slot], ctx->stream));
+    ctx->launches += w->nodes[slot];
+    CU(cudaMemcpyAsync(S, w->st, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> fin(nrhs, 0);
+    bool any = false;
+    for (int k = 0; k < nrhs; k++)
+      {
+        w->mask_h[k].stop = 1;
+        if (b->state[k] != SLOT_RUNNING || S[k].stop == STOP_RUN) continue;
+        if (S[k].stop == STOP_BREAKDOWN)
+          {
+            b->status[k] = TMS_ERR_NAN;
+            fin[k] = 1;
+            continue;
+          }
+        w->mask_h[k].stop = 0; // final residual (FP64) or reliable update (mixed)
+        any = true;
+      }
+    if (any)
+      {
+        CU(cudaMemcpyAsync(w->mask, w->mask_h, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
+        std::vector<double> rr(nrhs, 0.0);
+        if (!mixed)
+          {
+            // the FP64 iteration accumulated x in the inner field
+            ++ctx->launches;
+            axpby_mrhs_kernel<PREC_F64, PX, PX><<<bg, 256, 0, ctx->stream>>>(
+              n, nrhs, 1.0, bview<PX>(w->xlo), 0.0, bview<PX>(w->xlo), bview<PREC_F64>(w->hi[1]), w->mask);
+            TRY(true_residual_b(ctx, w, nrhs, w->hi[1], rr.data()));
+            for (int k = 0; k < nrhs; k++)
+              if (!w->mask_h[k].stop)
+                {
+                  b->tres[k] = rr[k];
+                  b->status[k] = (S[k].stop == STOP_MAXITER) ? TMS_ERR_NOT_CONVERGED : TMS_OK;
+                  fin[k] = 1;
+                }
+          }
+        else
+          {
+            // x += x_lo ; x_lo = 0 ; r = b - A x   (FP64, masked)
+            ctx->launches += 2;
+            axpby_mrhs_kernel<PREC_F64, PREC_F64, PX><<<bg, 256, 0, ctx->stream>>>(
+              n, nrhs, 1.0, bview<PREC_F64>(w->hi[1]), 1.0, bview<PX>(w->xlo), bview<PREC_F64>(w->hi[1]), w->mask);
+            axpby_mrhs_kernel<PX, PX, PX><<<bg, 256, 0, ctx->stream>>>(n, nrhs, 0.0, bview<PX>(w->xlo), 0.0,
+                                                                       bview<PX>(w->xlo), bview<PX>(w->xlo), w->mask);
+            TRY(true_residual_b(ctx, w, nrhs, w->hi[1], rr.data()));
+            bool restart = false;
+            for (int k = 0; k < nrhs; k++)
+              {
+                if (w->mask_h[k].stop) continue;
+                b->reliable[k]++;
+                b->tres[k] = rr[k];
+                if (rr[k] < S[k].target || S[k].stop == STOP_MAXITER || S[k].iter >= b->niter[k])
+                  {
+                    b->status[k] = (rr[k] < S[k].target) ? TMS_OK : TMS_ERR_NOT_CONVERGED;
+                    fin[k] = 1;
+                    w->mask_h[k].stop = 1;
+                    continue;
+                  }
+                S[k].beta = rr[k] / S[k].rr_prev;
+                S[k].rr = rr[k];
+                S[k].rel_trigger = delta * delta * rr[k];
+                S[k].stop = STOP_RUN;
+                restart = true;
+              }
+            if (restart)
+              {
+                CU(cudaMemcpyAsync(w->mask, w->mask_h, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
+                // r_lo = r ; p_lo = r_lo + beta p_lo   (masked)
+                ++ctx->launches;
+                axpby_mrhs_kernel<P, PREC_F64, PREC_F64><<<bg, 256, 0, ctx->stream>>>(
+                  n, nrhs, 1.0, bview<PREC_F64>(w->hi[2]), 0.0, bview<PREC_F64>(w->hi[2]), bview<P>(w->lo[1]),
+                  w->mask);
+                CU(cudaMemcpyAsync(w->st, S, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
+                ++ctx->launches;
+                xpay_mrhs_kernel<P><<<bg, 256, 0, ctx->stream>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]), w->st,
+                                                                 w->mask);
+              }
+          }
+      }
+    const auto now = std::chrono::steady_clock::now();
+    bool changed = false;
+    for (int k = 0; k < nrhs; k++)
+      {
+        finished[k] = fin[k];
+        if (!fin[k]) continue;
+        S[k].stop = STOP_IDLE;
+        b->state[k] = SLOT_FINISHED;
+        b->secs[k] = std::chrono::duration<double>(now - b->t0[k]).count();
+        changed = true;
+      }
+    if (changed || any) CU(cudaMemcpyAsync(w->st, S, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(ctx->stream));
+    return TMS_OK;
+  }
+}
+
+extern "C" {
+
+tms_status tms_batch_open(tms_ctx* ctx, int nslots, int precision, int has_anis, double anis, tms_batch** out)
+{
+  if (!out) return TMS_ERR_BAD_ARG;
+  *out = nullptr;
+  TRY(check_conf(ctx));
+  if (nslots <= 0 || nslots > MRHS_MAX) return fail(ctx, TMS_ERR_BAD_ARG, "nslots: 1..%d", MRHS_MAX);
+  if (precision != TMS_PREC_DOUBLE && precision != TMS_PREC_MIXED_SINGLE && precision != TMS_PREC_MIXED_HALF)
+    return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
+  BatchWork* w;
+  TRY(work(ctx, &w));
+  if (w->open) return fail(ctx, TMS_ERR_BAD_ARG, "a batch session is already open on this context");
+  tms_batch* b = new tms_batch;
+  b->ctx = ctx;
+  b->w = w;
+  b->nslots = nslots;
+  b->prec = precision;
+  b->has_anis = has_anis;
+  b->anis = has_anis ? anis : 1.0;
+  b->state.assign(nslots, SLOT_FREE);
+  b->b2.assign(nslots, 0.0);
+  b->tres.assign(nslots, 0.0);
+  b->reliable.assign(nslots, 0);
+  b->niter.assign(nslots, 0);
+  b->status.assign(nslots, TMS_OK);
+  b->t0.assign(nslots, std::chrono::steady_clock::now());
+  b->secs.assign(nslots, 0.0);
+  const tms_status st = open_fields(b);
+  if (st != TMS_OK)
+    {
+      delete b;
+      return st;
+    }
+  for (int k = 0; k < nslots; k++)
+    {
+      memset(&w->st_h[k], 0, sizeof(CgState));
+      w->st_h[k].stop = STOP_IDLE;
+      w->bp_h->kappa[k] = 0.125;
+      w->bp_h->mu[k] = 0.0;
+    }
+  w->bp_h->anis = b->anis;
+  CU(cudaMemcpyAsync(w->st, w->st_h, sizeof(CgState) * nslots, cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(w->bp, w->bp_h, sizeof(BatchParams), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  w->open = true;
+  *out = b;
+  return TMS_OK;
+}
+
+tms_status tms_batch_submit(tms_batch* b, int slot, const double* src_lx, double kappa, double mu, int niter,
+                            double residue)
+{
+  if (!b) return TMS_ERR_BAD_ARG;
+  tms_ctx* ctx = b->ctx;
+  TRY(check_conf(ctx));
+  if (slot < 0 || slot >= b->nslots || b->state[slot] != SLOT_FREE)
+    return fail(ctx, TMS_ERR_BAD_ARG, "slot %d is not free", slot);
+  if (!src_lx || niter <= 0 || !(residue > 0) || !(kappa > 0) || !std::isfinite(mu))
+    return fail(ctx, TMS_ERR_BAD_ARG, "bad right-hand side arguments");
+  BatchWork* w = b->w;
+  w->bp_h->kappa[slot] = kappa;
+  w->bp_h->mu[slot] = mu;
+  // Eq. (8): varphi -> hi[0][slot], eta_e -> hi[6][slot] (single-RHS FP64 kernels)
+  TRY(set_params(ctx, kappa, mu, b->has_anis, b->anis));
+  Field* f = ctx->f64;
+  for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
+  for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
+  const int64_t Vh = ctx->g.Vh;
+  const int n = (int)Vh;
+  const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
+  const double* src = src_lx;
+  if (ctx->ptr_mode == TMS_PTR_HOST)
+    {
+      TRY(ensure_stage(ctx, bytes));
+      CU(cudaMemcpyAsync(ctx->stage, src_lx, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      src = ctx->stage;
+    }
+  auto V = [](const Field& x) { return view<PREC_F64>(x); };
+  const Field ek = one(w->hi[6], slot), vk = one(w->hi[0], slot);
+  ctx->launches += 3;
+  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(ek));
+  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(ctx->ex[1]));
+  diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(ek), V(f[5]), ctx->prm, 1.0, 1);
+  EpiSrcPrep<PREC_F64> sp{{V(vk), V(vk)}, {V(ctx->ex[1]), V(ctx->ex[1])}};
+  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], links64(ctx), ctx->prm, sp);
+  CU(cudaGetLastError());
+  tms_status st;
+  if (b->prec == TMS_PREC_DOUBLE) st = session_submit<PREC_F64>(b, slot, residue, niter);
+  else if (b->prec == TMS_PREC_MIXED_SINGLE) st = session_submit<PREC_F32>(b, slot, residue, niter);
+  else st = session_submit<PREC_F16>(b, slot, residue, niter);
+  if (st != TMS_OK) return st;
+  CU(cudaStreamSynchronize(ctx->stream));
+  b->state[slot] = SLOT_RUNNING;
+  b->t0[slot] = std::chrono::steady_clock::now();
+  return TMS_OK;
+}
+
+tms_status tms_batch_step(tms_batch* b, int* finished, int* nfinished)
+{
+  if (!b || !finished) return TMS_ERR_BAD_ARG;
+  tms_ctx* ctx = b->ctx;
+  TRY(check_conf(ctx));
+  int running = 0;
+  for (int k = 0; k < b->nslots; k++)
+    {
+      finished[k] = 0;
+      running += (b->state[k] == SLOT_RUNNING);
+    }
+  if (nfinished) *nfinished = 0;
+  if (!running) return TMS_OK;
+  tms_status st;
+  if (b->prec == TMS_PREC_DOUBLE) st = session_step<PREC_F64>(b, links64(ctx), finished);
+  else if (b->prec == TMS_PREC_MIXED_SINGLE)
+    st = ctx->su3 ? session_step<PREC_F32>(b, links32r(ctx), finished)
+                  : session_step<PREC_F32>(b, links32f(ctx), finished);
+  else
+    st = ctx->su3 ? session_step<PREC_F16>(b, links16r(ctx), finished)
+                  : session_step<PREC_F16>(b, links32f(ctx), finished);
+  if (st != TMS_OK) return st;
+  if (nfinished)
+    for (int k = 0; k < b->nslots; k++) *nfinished += finished[k];
+  return TMS_OK;
+}
+
+tms_status tms_batch_collect(tms_batch* b, int slot, double* sol_lx, tms_stats* stats)
+{
+  if (!b) return TMS_ERR_BAD_ARG;
+  tms_ctx* ctx = b->ctx;
+  TRY(check_conf(ctx));
+  if (slot < 0 || slot >= b->nslots || b->state[slot] != SLOT_FINISHED)
+    return fail(ctx, TMS_ERR_BAD_ARG, "slot %d has no finished solution", slot);
+  if (!sol_lx) return fail(ctx, TMS_ERR_BAD_ARG, "null solution buffer");
+  BatchWork* w = b->w;
+  const double kappa = w->bp_h->kappa[slot], mu = w->bp_h->mu[slot];
+  TRY(set_params(ctx, kappa, mu, b->has_anis, b->anis));
+  Field* f = ctx->f64;
+  Field* psi = ctx->ex + 2;
+  const int64_t Vh = ctx->g.Vh;
+  const int n = (int)Vh;
+  const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
+  auto U = links64(ctx);
+  auto V = [](const Field& x) { return view<PREC_F64>(x); };
+  // Eq. (10)-(11) and paste
+  const Field xk = one(w->hi[1], slot), ek = one(w->hi[6], slot);
+  kern_op<PREC_F64>(ctx, U, xk, f[5], psi[1], -1.0, ctx->prm);
+  EpiReco<PREC_F64> rc{{V(psi[0]), V(psi[0])}, {V(ek), V(ek)}, ctx->prm, 1.0};
+  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
+  double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sol_lx;
+  if (ctx->ptr_mode == TMS_PTR_HOST) TRY(ensure_stage(ctx, bytes));
+  d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sol_lx;
+  ctx->launches += 2;
+  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, d);
+  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, d);
+  CU(cudaGetLastError());
+  if (ctx->ptr_mode == TMS_PTR_HOST) CU(cudaMemcpyAsync(sol_lx, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  TRY(finish(ctx));
+  const CgState& S = w->st_h[slot];
+  if (stats)
+    {
+      stats->status = b->status[slot];
+      stats->iterations = S.iter;
+      stats->reliable_updates = b->reliable[slot];
+      stats->iterated_rel_res2 = S.rr / b->b2[slot];
+      stats->true_rel_res2 = b->tres[slot] / b->b2[slot];
+      stats->lx_rel_res2 = 0.0;
+      stats->seconds = b->secs[slot];
+    }
+  b->state[slot] = SLOT_FREE;
+  return b->status[slot];
+}
+
+tms_status tms_batch_close(tms_batch* b)
+{
+  if (!b) return TMS_OK;
+  b->w->open = false;
+  delete b;
+  return TMS_OK;
+}
+
+tms_status tms_cg_eoprec_batched(tms_ctx* ctx, int nrhs, double* const* sols_lx, const double* const* srcs_lx,
+                                 double kappa, int has_anis, double anis, const double* mus, int niter,
+                                 const double* residues, int precision, tms_stats* stats)
+{
+  TRY(check_conf(ctx));
+  if (nrhs <= 0 || nrhs > MRHS_MAX || !sols_lx || !srcs_lx || !mus || !residues || niter <= 0)
+    return fail(ctx, TMS_ERR_BAD_ARG, "bad batched arguments (1 <= nrhs <= %d)", MRHS_MAX);
+  for (int k = 0; k < nrhs; k++)
+    if (!sols_lx[k] || !srcs_lx[k] || !(residues[k] > 0) || !std::isfinite(mus[k]))
+      return fail(ctx, TMS_ERR_BAD_ARG, "bad right-hand side %d", k);
+  tms_batch* b = nullptr;
+  TRY(tms_batch_open(ctx, nrhs, precision, has_anis, anis, &b));
+  struct Closer
+  {
+    tms_batch* b;
+    ~Closer() { tms_batch_close(b); }
+  } closer{b};
+  for (int k = 0; k < nrhs; k++)
+    {
+      const tms_status s = tms_batch_submit(b, k, srcs_lx[k], kappa, mus[k], niter, residues[k]);
+      if (s != TMS_OK) return s;
+    }
+  std::vector<int> fin(nrhs);
+  int left = nrhs;
+  tms_status worst = TMS_OK;
+  while (left > 0)
+    {
+      int nf = 0;
+      TRY(tms_batch_step(b, fin.data(), &nf));
+      for (int k = 0; k < nrhs; k++)
+        if (fin[k])
+          {
+            const tms_status s = tms_batch_collect(b, k, sols_lx[k], stats ? stats + k : nullptr);
+            if (s != TMS_OK && s != TMS_ERR_NOT_CONVERGED && s != TMS_ERR_NAN) return s;
+            if (s != TMS_OK && worst == TMS_OK) worst = s;
+            left--;
+          }
+    }
+  if (worst == TMS_ERR_NAN) return fail(ctx, worst, "nanned");
+  if (worst == TMS_ERR_NOT_CONVERGED) return fail(ctx, worst, "exit without converging");
+  return TMS_OK;
+}
+
+} // extern "C"

@@ -1,12 +1,10 @@
 // Multi-RHS kernels: k right-hand sides, each with its own twisted mass and
 // its own CG scalars, share one pass over the gauge links.
 //
-// Launch shape: persistent blocks of 8 warps walk the lattice 32 sites at a
-// time; for each 32-site chunk warp w takes the right-hand sides w, w+8, ...
-// All warps of a block read the same links for the same sites, so the links
-// cross HBM about once per chunk and are served to the other right-hand sides
-// from L1; each right-hand side's spinors are read by one warp as contiguous
-// 128-bit segments.
+// A warp takes 32 consecutive sites and, one group after the other, the
+// right-hand sides in groups of R (R per thread, in registers), so each link
+// is loaded once per group and applied to R spinors; each right-hand side's
+// spinors are read as contiguous 128-bit segments.
 //
 // Reductions are per right-hand side: a block accumulates each right-hand
 // side's warp sums in shared memory, writes one partial per block, and the
@@ -36,9 +34,12 @@ namespace tms
     }
   };
 
+  // per right-hand side hopping parameter and twisted mass (the hop itself
+  // does not depend on them: only the diagonal terms do)
   struct BatchParams
   {
-    double kappa, anis;
+    double anis;
+    double kappa[MRHS_MAX];
     double mu[MRHS_MAX];
   };
 
@@ -106,7 +107,7 @@ namespace tms
                                                  C<typename SpinorT<P>::R> acc[12]) const
     {
       using R = typename SpinorT<P>::R;
-      const OpParams o{bp.kappa, bp.mu[r], bp.anis};
+      const OpParams o{bp.kappa[r], bp.mu[r], bp.anis};
       const C<R> z = zinvdiag<R>(o, sgn);
 #pragma unroll
       for (int c = 0; c < 12; c++) acc[c] = diag_apply(acc[c], z, c);
@@ -125,7 +126,7 @@ namespace tms
                                                  C<typename SpinorT<P>::R> acc[12]) const
     {
       using R = typename SpinorT<P>::R;
-      const OpParams o{bp.kappa, bp.mu[r], bp.anis};
+      const OpParams o{bp.kappa[r], bp.mu[r], bp.anis};
       const C<R> z = zdiag<R>(o, sgn);
       C<R> xv[12];
       x.rhs(r).load(ieo, xv);
@@ -157,7 +158,7 @@ namespace tms
     {
       using R = typename SpinorT<P>::R;
       using RX = typename SpinorT<PX>::R;
-      const OpParams o{bp.kappa, bp.mu[k], bp.anis};
+      const OpParams o{bp.kappa[k], bp.mu[k], bp.anis};
       const C<R> z = zdiag<R>(o, sgn);
       const double a = st[k].alpha;
       const R alpha = R(a);

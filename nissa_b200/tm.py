@@ -70,6 +70,68 @@ class _Buf:
                 a.numel() if _is_torch(a) else a.size, tuple(shape)))
 
 
+class BatchSession:
+    """Continuous batching on one lattice (tms_batch_* of the C ABI): up to
+    ``nslots`` inv_tmD_cg_eoprec solves in flight, each with its own kappa,
+    mu and residue; new right-hand sides are submitted into free slots while
+    others keep iterating.  Driven by one host thread."""
+
+    def __init__(self, lattice: "Lattice", nslots: int, precision: str = "single", anis=None):
+        self.lat = lattice
+        self.lib = lattice.lib
+        self.nslots = nslots
+        a = Lattice._anis(anis)
+        h = ctypes.c_void_p()
+        st = self.lib.tms_batch_open(lattice.h, int(nslots), PRECISION[precision], a[0], a[1], ctypes.byref(h))
+        lattice._check(st, "tms_batch_open")
+        self.h = h
+        self._fin = (ctypes.c_int * nslots)()
+        self._keep = {}
+
+    def free_slots(self):
+        return [k for k in range(self.nslots) if k not in self._keep]
+
+    def submit(self, slot: int, source_lx, kappa: float, mu: float, niter: int, residue: float):
+        b = _Buf(source_lx, (self.lat.V, 4, 3, 2))
+        self.lat._mode(b)
+        st = self.lib.tms_batch_submit(self.h, int(slot), b.ptr, float(kappa), float(mu), int(niter), float(residue))
+        self.lat._check(st, "tms_batch_submit")
+        self._keep[slot] = b
+
+    def step(self):
+        """One block of lock-step iterations; returns the slots that finished."""
+        nf = ctypes.c_int(0)
+        st = self.lib.tms_batch_step(self.h, self._fin, ctypes.byref(nf))
+        self.lat._check(st, "tms_batch_step")
+        return [k for k in range(self.nslots) if self._fin[k]]
+
+    def collect(self, slot: int, out=None):
+        """Solution of a finished slot (and frees it): returns (sol, stats)."""
+        like = self._keep[slot].keep
+        sol = self.lat._new_out(like, (self.lat.V, 4, 3, 2)) if out is None else out
+        o = _Buf(sol, (self.lat.V, 4, 3, 2), out=True)
+        self.lat._mode(o)
+        stats = _lib.Stats()
+        st = self.lib.tms_batch_collect(self.h, int(slot), o.ptr, ctypes.byref(stats))
+        del self._keep[slot]
+        if st not in (0, 1, 2):
+            self.lat._check(st, "tms_batch_collect")
+        d = stats.as_dict()
+        d["status"] = st
+        return sol, d
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tms_batch_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 class Lattice:
     """One T x LX x LY x LZ lattice with a resident gauge configuration on one GPU.
 
@@ -302,6 +364,9 @@ class Lattice:
         if raise_on_error:
             self._check(st, "inv_tmD_cg_eoprec_batched", sd, out)
         return out, sd
+
+    def batch_session(self, nslots: int, precision: str = "single", anis=None) -> BatchSession:
+        return BatchSession(self, nslots, precision, anis)
 
     def inv_tmD_cg_eoprec(self, kappa, mu, source_lx, niter, residue, anis=None, precision="double", out=None,
                           raise_on_error=True):

@@ -52,3 +52,38 @@ def test_batched_argument_errors(cuda_device):
         with pytest.raises(TmError) as e:
             lat.inv_tmD_cg_eoprec_batched(0.16, [0.01] * 65, [x] * 65, 100, 1e-20)
         assert e.value.status == 3
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_session_admits_while_running(cuda_device, precision):
+    """Continuous batching: right-hand sides with different kappa and mu are
+    submitted while others are iterating; every result equals its own single
+    solve."""
+    T, L = 8, 8
+    conf = wl.gauge_conf(T, L, 0.35, seed=61)
+    reqs = [(0.156 + 0.001 * k, 0.002 * (k + 1), wl.z2_source(T, L, 70 + k)) for k in range(7)]
+    res = 1e-20
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        refs = [lat.inv_tmD_cg_eoprec(kp, mu, s, 100000, 1e-24)[0] for kp, mu, s in reqs]
+        out = {}
+        with lat.batch_session(3, precision) as ses:
+            pending = list(range(len(reqs)))
+            running = {}
+            steps = 0
+            while pending or running:
+                for slot in ses.free_slots():
+                    if not pending:
+                        break
+                    k = pending.pop(0)
+                    kp, mu, s = reqs[k]
+                    ses.submit(slot, s, kp, mu, 100000, res)
+                    running[slot] = k
+                for slot in ses.step():
+                    sol, st = ses.collect(slot)
+                    assert st["status"] == 0 and st["true_rel_res2"] < res
+                    out[running.pop(slot)] = sol
+                steps += 1
+                assert steps < 10000
+        for k in range(len(reqs)):
+            assert rel(out[k], refs[k]) < 1e-9, k
