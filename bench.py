@@ -327,6 +327,8 @@ def run_kernel_only(args):
     conf = wl.gauge_conf(W["T"], W["L"], W["eps"], W["seed"], device="cuda:0")
     lat = Lattice(W["T"], W["L"], bc_t=W["bc_t"])
     lat.upload_conf(conf)
+    if args.hop_cfg >= 0:
+        lat.set_tuning("hop_cfg_" + args.kernel_only, args.hop_cfg)
     if args.nrhs > 1:
         if args.mrhs:
             lat.set_tuning("mrhs_per_thread", args.mrhs)
@@ -431,6 +433,7 @@ def main():
     ap.add_argument("--nrep", type=int, default=10, help="launches for --kernel-only")
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
+    ap.add_argument("--hop-cfg", type=int, default=-1, help="hopping-kernel launch shape for --kernel-only (tuning)")
     ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve"],
                     help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop (extra reports)")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (requests/s)")

@@ -181,11 +181,15 @@ tms_status tms_batch_close(tms_batch *batch);
 /* Number of CUDA kernels this context has launched (CUDA-graph replays count their nodes). */
 uint64_t tms_launch_count(const tms_ctx *ctx);
 /* Tuning knobs (no reference counterpart), used by the autotuner: "hop_cfg_double",
- * "hop_cfg_single", "hop_cfg_half" (hopping-kernel launch shape 0..2: 128 threads; 128 threads
- * with registers capped for 4 (FP64) / 8 resident blocks; 256 threads capped for 2 / 4),
+ * "hop_cfg_single", "hop_cfg_half" (hopping-kernel launch shape 0..2: one site per thread, 128 threads;
+ * 128 threads with registers capped for 4 (FP64) / 8 resident blocks; 256 threads capped for 2 / 4;
+ * single and half only, when T is a multiple of 4 (else shape 0 is used): 3 two sites (t, t+T/2) per
+ * thread in packed FP32 arithmetic with the neighbours streamed through shared memory by cp.async,
+ * 4 two sites per thread in packed FP32 arithmetic),
  * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
  * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
- * dropped by this factor, 0 < delta < 1), "mrhs_per_thread" (right-hand sides one thread of the
+ * dropped by this factor, 0 < delta < 1), "links_single" (0: the FP32-spinor inner solver reads FP32
+ * 12-real links, 1: 16-bit fixed-point 12-real links), "mrhs_per_thread" (right-hand sides one thread of the
  * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2).  Results do not depend on the launch shapes. */
 tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);
 /* Time the e/o hopping kernel alone with CUDA events on the context's stream: nrep launches,

@@ -396,8 +396,9 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
   if (k == "hop_cfg_double" || k == "hop_cfg_single" || k == "hop_cfg_half")
     {
       const int v = (int)value;
-      if (v < 0 || v >= HOP_CFGS || v != value) return fail(ctx, TMS_ERR_BAD_ARG, "%s: 0..%d", key, HOP_CFGS - 1);
       const int p = (k == "hop_cfg_double") ? PREC_F64 : (k == "hop_cfg_single") ? PREC_F32 : PREC_F16;
+      const int ncfg = (p == PREC_F64) ? HOP_CFGS : HOP_CFGS_ALL;
+      if (v < 0 || v >= ncfg || v != value) return fail(ctx, TMS_ERR_BAD_ARG, "%s: 0..%d", key, ncfg - 1);
       if (ctx->hop_cfg[p] != v) drop_all();
       ctx->hop_cfg[p] = v;
       return TMS_OK;
@@ -423,6 +424,13 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       ctx->mrhs_r = v;
       return TMS_OK;
     }
+  if (k == "links_single")
+    {
+      if (value != 0.0 && value != 1.0) return fail(ctx, TMS_ERR_BAD_ARG, "links_single: 0 (FP32) or 1 (16-bit)");
+      if (ctx->single_links16 != (int)value) drop_all();
+      ctx->single_links16 = (int)value;
+      return TMS_OK;
+    }
   if (k == "reliable_delta_single" || k == "reliable_delta_half")
     {
       if (!(value > 0.0 && value < 1.0)) return fail(ctx, TMS_ERR_BAD_ARG, "%s: in (0, 1)", key);
@@ -441,6 +449,9 @@ tms_status tms_bench_hop(tms_ctx* ctx, int precision, int variant, int nrep, int
   TRY(set_params(ctx, 0.16, 0.01, 0, 1.0));
   if (precision == TMS_PREC_DOUBLE)
     return bench_hop_t<PREC_F64>(ctx, links64(ctx), variant, nrep, flush, ms_per_launch, 144.0, 192.0,
+                                 bytes_per_launch);
+  if (precision == TMS_PREC_MIXED_SINGLE && ctx->su3 && ctx->single_links16)
+    return bench_hop_t<PREC_F32>(ctx, links16r(ctx), variant, nrep, flush, ms_per_launch, 24.0, 96.0,
                                  bytes_per_launch);
   if (precision == TMS_PREC_MIXED_SINGLE)
     return ctx->su3 ? bench_hop_t<PREC_F32>(ctx, links32r(ctx), variant, nrep, flush, ms_per_launch, 48.0, 96.0,

@@ -218,17 +218,19 @@ namespace tms
     bool w;
     const int n = FWD ? nbr_up<MU>(g, s, w) : nbr_dw<MU>(g, s, w);
     C<Re> L[9];
-    U.load(FWD ? p : 1 - p, MU, FWD ? ieo : n, L);
-    const Re f = w ? fmu * Re(g.bc_t) : fmu;
+    Re ls;
+    U.load_scaled(FWD ? p : 1 - p, MU, FWD ? ieo : n, L, ls);
+    const Re f = (w ? fmu * Re(g.bc_t) : fmu) * ls;
 #pragma unroll
     for (int j = 0; j < R; j++)
       if (on & (1u << j))
         {
           C<Re> sp[12], h0[3], h1[3], u0[3], u1[3];
-          in.rhs(rhs0 + j).load(n, sp);
+          Re ss;
+          in.rhs(rhs0 + j).load_raw(n, sp, ss);
           project<MU, FWD>(sp, h0, h1);
-          link_mul<FWD>(L, h0, u0, f);
-          link_mul<FWD>(L, h1, u1, f);
+          link_mul<FWD>(L, h0, u0, f * ss);
+          link_mul<FWD>(L, h1, u1, f * ss);
           reconstruct<MU, FWD>(acc[j], u0, u1);
         }
   }

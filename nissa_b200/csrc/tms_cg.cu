@@ -283,6 +283,7 @@ namespace
     int reliable = 0;
     float ms = 0;
     tms_status st = TMS_OK;
+    double last_rt = have_guess ? rr : -1.0; // true residual of the current x, if known
     if (rr >= target)
       {
         convert<P, PREC_F64>(ctx, f[2], lo[1], 1.0, n); // r_lo = r
@@ -319,6 +320,7 @@ namespace
             double rt;
             TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rt));
             reliable++;
+            last_rt = rt; // the true residual of the current x
             if (rt < target) break;
             if (S.stop == STOP_MAXITER || S.iter >= niter)
               {
@@ -342,8 +344,9 @@ namespace
         CU(cudaEventSynchronize(ctx->ev1));
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
       }
-    double tr;
-    TRY(Op::true_residual(ctx, f[0], f[1], f[6], &tr));
+    // the last reliable update left x with its FP64 true residual; otherwise recompute it
+    double tr = last_rt;
+    if (tr < 0.0) TRY(Op::true_residual(ctx, f[0], f[1], f[6], &tr));
     fill_stats(stats, st, S.iter, reliable, S.rr / b2, tr / b2, ms);
     return st;
   }
@@ -353,8 +356,11 @@ namespace
   {
     if (precision == TMS_PREC_DOUBLE) return cg_double<Op>(ctx, niter, residue, have_guess, stats);
     if (precision == TMS_PREC_MIXED_SINGLE)
-      return ctx->su3 ? cg_mixed<Op, PREC_F32>(ctx, links32r(ctx), niter, residue, have_guess, stats)
-                      : cg_mixed<Op, PREC_F32>(ctx, links32f(ctx), niter, residue, have_guess, stats);
+      {
+        if (!ctx->su3) return cg_mixed<Op, PREC_F32>(ctx, links32f(ctx), niter, residue, have_guess, stats);
+        return ctx->single_links16 ? cg_mixed<Op, PREC_F32>(ctx, links16r(ctx), niter, residue, have_guess, stats)
+                                   : cg_mixed<Op, PREC_F32>(ctx, links32r(ctx), niter, residue, have_guess, stats);
+      }
     if (precision == TMS_PREC_MIXED_HALF)
       return ctx->su3 ? cg_mixed<Op, PREC_F16>(ctx, links16r(ctx), niter, residue, have_guess, stats)
                       : cg_mixed<Op, PREC_F16>(ctx, links32f(ctx), niter, residue, have_guess, stats);

@@ -131,6 +131,12 @@ namespace tms
     double2* __restrict__ d;
     float* __restrict__ n; // unused
     int stride;
+    // values and a scale to apply to them (1 here: the values are exact)
+    __device__ __forceinline__ void load_raw(int site, C<double> v[12], double& scale) const
+    {
+      load(site, v);
+      scale = 1.0;
+    }
     __device__ __forceinline__ void load(int site, C<double> v[12]) const
     {
 #pragma unroll
@@ -153,6 +159,11 @@ namespace tms
     float4* __restrict__ d;
     float* __restrict__ n; // unused
     int stride;
+    __device__ __forceinline__ void load_raw(int site, C<float> v[12], float& scale) const
+    {
+      load(site, v);
+      scale = 1.0f;
+    }
     __device__ __forceinline__ void load(int site, C<float> v[12]) const
     {
 #pragma unroll
@@ -177,6 +188,24 @@ namespace tms
     uint4* __restrict__ d;
     float* __restrict__ n;
     int stride;
+    // the stored halves and the per-site factor that scales them
+    __device__ __forceinline__ void load_raw(int site, C<float> v[12], float& scale) const
+    {
+      scale = __ldg(n + site);
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        {
+          const uint4 w = __ldg(d + (size_t)k * stride + site);
+          const unsigned u[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            {
+              __half2 h = *reinterpret_cast<const __half2*>(&u[j]);
+              const float2 f = __half22float2(h);
+              v[4 * k + j] = {f.x, f.y};
+            }
+        }
+    }
     __device__ __forceinline__ void load(int site, C<float> v[12]) const
     {
       const float s = __ldg(n + site);
@@ -227,6 +256,12 @@ namespace tms
     using R = double;
     const double2* __restrict__ d; // [par][mu][9][Vh]
     int Vh;
+    // the link and a factor to apply to its products (1 here)
+    __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<double> u[9], double& scale) const
+    {
+      load(par, mu, site, u);
+      scale = double(1);
+    }
     __device__ __forceinline__ void load(int par, int mu, int site, C<double> u[9]) const
     {
       const double2* b = d + ((size_t)(par * 4 + mu) * 9) * Vh + site;
@@ -244,6 +279,16 @@ namespace tms
     using R = float;
     const float2* __restrict__ d; // [par][mu][9][Vh]
     int Vh;
+    // the link and a factor to apply to its products (1 here)
+    __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<float> u[9], float& scale) const
+    {
+      load(par, mu, site, u);
+      scale = float(1);
+    }
+    // stored rows (all three) in stored units, for the two-site kernels
+    static constexpr int kRows = 3;
+    static constexpr float kUnit = 1.0f;
+    __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[9]) const { load(par, mu, site, u); }
     __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
     {
       const float2* b = d + ((size_t)(par * 4 + mu) * 9) * Vh + site;
@@ -261,6 +306,26 @@ namespace tms
     using R = float;
     const float4* __restrict__ d; // [par][mu][3][Vh]
     int Vh;
+    // the link and a factor to apply to its products (1 here)
+    __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<float> u[9], float& scale) const
+    {
+      load(par, mu, site, u);
+      scale = float(1);
+    }
+    // stored rows 0 and 1 in stored units, for the two-site kernels
+    static constexpr int kRows = 2;
+    static constexpr float kUnit = 1.0f;
+    __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[6]) const
+    {
+      const float4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
+      const float4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      u[0] = {a0.x, a0.y};
+      u[1] = {a0.z, a0.w};
+      u[2] = {a1.x, a1.y};
+      u[3] = {a1.z, a1.w};
+      u[4] = {a2.x, a2.y};
+      u[5] = {a2.z, a2.w};
+    }
     __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
     {
       const float4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
@@ -283,6 +348,38 @@ namespace tms
     using R = float;
     const short4* __restrict__ d; // [par][mu][3][Vh]
     int Vh;
+    // stored rows 0 and 1 in raw 16-bit units (value = raw * kUnit), for the two-site kernels
+    static constexpr int kRows = 2;
+    static constexpr float kUnit = 1.0f / 32767.0f;
+    __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[6]) const
+    {
+      const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
+      const short4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      u[0] = {float(a0.x), float(a0.y)};
+      u[1] = {float(a0.z), float(a0.w)};
+      u[2] = {float(a1.x), float(a1.y)};
+      u[3] = {float(a1.z), float(a1.w)};
+      u[4] = {float(a2.x), float(a2.y)};
+      u[5] = {float(a2.z), float(a2.w)};
+    }
+    // rows 0 and 1 in raw 16-bit units, row 2 rebuilt from them and brought to
+    // the same units: the products of this link are to be multiplied by `scale`
+    __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<float> u[9], float& scale) const
+    {
+      constexpr float k = 1.0f / 32767.0f;
+      const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
+      const short4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      u[0] = {float(a0.x), float(a0.y)};
+      u[1] = {float(a0.z), float(a0.w)};
+      u[2] = {float(a1.x), float(a1.y)};
+      u[3] = {float(a1.z), float(a1.w)};
+      u[4] = {float(a2.x), float(a2.y)};
+      u[5] = {float(a2.z), float(a2.w)};
+      u[6] = cscale(cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4]))), k);
+      u[7] = cscale(cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5]))), k);
+      u[8] = cscale(cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3]))), k);
+      scale = k;
+    }
     __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
     {
       constexpr float k = 1.0f / 32767.0f;

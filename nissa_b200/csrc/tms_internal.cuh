@@ -4,6 +4,7 @@
 #pragma once
 #include "tmsolve.h"
 #include "tms_kernels.cuh"
+#include "tms_pipe.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -105,6 +106,7 @@ struct tms_ctx
   // reliable-update trigger of the mixed solvers
   int hop_cfg[3] = {0, 1, 0};
   double delta_single = 1e-3, delta_half = 0.005;
+  int single_links16 = 0; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
   int mrhs_r = 4; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
 
   // batched-solver workspace (owned by tms_batch.cu)
@@ -203,6 +205,24 @@ namespace tms_int
   {
     const int nsite = (int)(npar * c->g.Vh);
     ++c->launches;
+    if constexpr (P != PREC_F64)
+      if (c->hop_cfg[P] >= HOP_CFGS && c->g.T % 4 == 0)
+        {
+          const int n2 = nsite / 2;
+          if (c->hop_cfg[P] == 4)
+            hop2_kernel<P, LF, Epi, Fin><<<div_up(n2, HOP2_THREADS), HOP2_THREADS, 0, s>>>(
+              c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+          else
+            {
+              constexpr int smem = PipeFmt<P, LF>::SMEM;
+              static const cudaError_t attr = cudaFuncSetAttribute(
+                hop_pipe_kernel<P, LF, Epi, Fin>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+              (void)attr;
+              hop_pipe_kernel<P, LF, Epi, Fin><<<div_up(n2, PIPE_THREADS), PIPE_THREADS, smem, s>>>(
+                c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+            }
+          return;
+        }
     switch (c->hop_cfg[P])
       {
       case 1:

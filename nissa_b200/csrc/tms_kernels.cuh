@@ -166,6 +166,9 @@ namespace tms
       }
   }
 
+  // One direction of the stencil.  The factors of the hop (anisotropy, the
+  // time-boundary sign, the FP16 per-site scale of the neighbour, the 16-bit
+  // link scale) are folded into one multiplication of the two link products.
   template <int MU, int P, int LF>
   __device__ __forceinline__ void hop_dir(const Lattice& g, const Site& s, int p, int ieo, const SpinorT<P>& in,
                                           const LinkT<LF>& U, typename SpinorT<P>::R anis,
@@ -177,10 +180,11 @@ namespace tms
       bool w;
       const int n = nbr_up<MU>(g, s, w);
       C<R> sp[12], h0[3], h1[3], u0[3], u1[3], L[9];
-      in.load(n, sp);
+      R ss, ls;
+      in.load_raw(n, sp, ss);
       project<MU, true>(sp, h0, h1);
-      U.load(p, MU, ieo, L);
-      const R f = w ? fmu * R(g.bc_t) : fmu;
+      U.load_scaled(p, MU, ieo, L, ls);
+      const R f = (w ? fmu * R(g.bc_t) : fmu) * ss * ls;
       link_mul<true>(L, h0, u0, f);
       link_mul<true>(L, h1, u1, f);
       reconstruct<MU, true>(acc, u0, u1);
@@ -189,10 +193,11 @@ namespace tms
       bool w;
       const int n = nbr_dw<MU>(g, s, w);
       C<R> sp[12], h0[3], h1[3], u0[3], u1[3], L[9];
-      in.load(n, sp);
+      R ss, ls;
+      in.load_raw(n, sp, ss);
       project<MU, false>(sp, h0, h1);
-      U.load(1 - p, MU, n, L);
-      const R f = w ? fmu * R(g.bc_t) : fmu;
+      U.load_scaled(1 - p, MU, n, L, ls);
+      const R f = (w ? fmu * R(g.bc_t) : fmu) * ss * ls;
       link_mul<false>(L, h0, u0, f);
       link_mul<false>(L, h1, u1, f);
       reconstruct<MU, false>(acc, u0, u1);
@@ -711,7 +716,9 @@ namespace tms
     static constexpr int NT = (CFG == 2) ? 256 : 128;
     static constexpr int MINB = (CFG == 0) ? 1 : (CFG == 1) ? (P == PREC_F64 ? 4 : 8) : (P == PREC_F64 ? 2 : 4);
   };
-  constexpr int HOP_CFGS = 3;
+  constexpr int HOP_CFGS = 3;      // launch shapes of the one-site kernel
+  constexpr int HOP_CFGS_ALL = 5;  // FP32 arithmetic, T % 4 == 0: 3 the two-site packed kernel with
+                                   // the cp.async pipeline, 4 the two-site packed kernel
 
   template <int P, int LF, class Epi, class Fin, int CFG = 0>
   __global__ void __launch_bounds__(HopCfg<P, CFG>::NT, HopCfg<P, CFG>::MINB)
@@ -738,6 +745,222 @@ namespace tms
         part = epi(p, ieo, acc);
       }
     if (Epi::kReduce) grid_reduce<NT>(part, red, fin);
+  }
+
+  // ------------------------------------------- two sites per thread, packed
+  // For the FP32-arithmetic hops (FP32 and FP16 spinors) one thread computes
+  // the sites (t,x,y,z) and (t+T/2,x,y,z), t < T/2.  When T/2 is even the two
+  // have the same parity, e/o indices ieo and ieo + Vh/2, and the same spatial
+  // neighbour offsets.  Each real of the first site sits in lane x and the same
+  // real of the second in lane y of a float2, so the stencil runs on Blackwell's
+  // packed FP32 instructions (two lanes per instruction), halving the
+  // floating-point instruction count that bounds the low-precision hops.
+  struct P2
+  {
+    float2 v;
+  };
+  __device__ __forceinline__ P2 p2(float a, float b) { return {make_float2(a, b)}; }
+  __device__ __forceinline__ P2 operator+(P2 a, P2 b) { return {__fadd2_rn(a.v, b.v)}; }
+  __device__ __forceinline__ P2 operator-(P2 a) { return {make_float2(-a.v.x, -a.v.y)}; }
+  __device__ __forceinline__ P2 operator-(P2 a, P2 b) { return {__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y))}; }
+  __device__ __forceinline__ P2 operator*(P2 a, P2 b) { return {__fmul2_rn(a.v, b.v)}; }
+  __device__ __forceinline__ P2 fma2(P2 a, P2 b, P2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+
+  __device__ __forceinline__ C<P2> zip(C<float> a, C<float> b) { return {p2(a.re, b.re), p2(a.im, b.im)}; }
+
+  // an element of row 2 of a special-unitary link, conj(a d - b c), packed
+  __device__ __forceinline__ C<P2> row2_elem(C<P2> a, C<P2> b, C<P2> c, C<P2> d)
+  {
+    // conj(a d - b c)
+    P2 re = a.re * d.re;
+    re = fma2(-a.im, d.im, re);
+    re = fma2(-b.re, c.re, re);
+    re = fma2(b.im, c.im, re);
+    P2 im = (-a.re) * d.im;
+    im = fma2(-a.im, d.re, im);
+    im = fma2(b.re, c.im, im);
+    im = fma2(b.im, c.re, im);
+    return {re, im};
+  }
+
+  // link of site a (lane x) and site b (lane y) in stored units; its products
+  // are to be multiplied by LinkT::kUnit
+  template <int LF>
+  __device__ __forceinline__ void load_link2(const LinkT<LF>& U, int par, int mu, int sa, int sb, C<P2> L[9])
+  {
+    constexpr int NR = LinkT<LF>::kRows;
+    C<float> a[3 * NR], b[3 * NR];
+    U.load_rows(par, mu, sa, a);
+    U.load_rows(par, mu, sb, b);
+#pragma unroll
+    for (int k = 0; k < 3 * NR; k++) L[k] = zip(a[k], b[k]);
+    if (NR == 2)
+      {
+        L[6] = row2_elem(L[1], L[2], L[4], L[5]);
+        L[7] = row2_elem(L[2], L[0], L[5], L[3]);
+        L[8] = row2_elem(L[0], L[1], L[3], L[4]);
+        // in stored units: the products of two stored values carry one unit too many
+        if (LinkT<LF>::kUnit != 1.0f)
+          {
+            const P2 unit = p2(LinkT<LF>::kUnit, LinkT<LF>::kUnit);
+#pragma unroll
+            for (int k = 6; k < 9; k++) L[k] = {L[k].re * unit, L[k].im * unit};
+          }
+      }
+  }
+
+  // u = U h (FWD) or U^+ h (backward), packed
+  template <bool FWD>
+  __device__ __forceinline__ void link_mul2(const C<P2> U[9], const C<P2> h[3], C<P2> u[3])
+  {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+      {
+        C<P2> a;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+          {
+            const C<P2> w = FWD ? U[3 * i + j] : U[3 * j + i];
+            const P2 wim = FWD ? w.im : -w.im;
+            if (j == 0)
+              {
+                a.re = w.re * h[j].re;
+                a.im = w.re * h[j].im;
+              }
+            else
+              {
+                a.re = fma2(w.re, h[j].re, a.re);
+                a.im = fma2(w.re, h[j].im, a.im);
+              }
+            a.re = fma2(-wim, h[j].im, a.re);
+            a.im = fma2(wim, h[j].re, a.im);
+          }
+        u[i] = a;
+      }
+  }
+
+  // acc += f u, acc -= f u, acc += i f u, acc -= i f u (nf = -f)
+  __device__ __forceinline__ void acc_add(C<P2>& acc, C<P2> u, P2 f, P2 nf)
+  {
+    acc.re = fma2(f, u.re, acc.re);
+    acc.im = fma2(f, u.im, acc.im);
+  }
+  __device__ __forceinline__ void acc_sub(C<P2>& acc, C<P2> u, P2 f, P2 nf) { acc_add(acc, u, nf, f); }
+  __device__ __forceinline__ void acc_iadd(C<P2>& acc, C<P2> u, P2 f, P2 nf)
+  {
+    acc.re = fma2(nf, u.im, acc.re);
+    acc.im = fma2(f, u.re, acc.im);
+  }
+  __device__ __forceinline__ void acc_isub(C<P2>& acc, C<P2> u, P2 f, P2 nf) { acc_iadd(acc, u, nf, f); }
+
+  // the reconstruction of `reconstruct`, with the hop factor folded into its fused multiply-adds
+  template <int MU, bool FWD>
+  __device__ __forceinline__ void reconstruct2(C<P2> acc[12], const C<P2> u0[3], const C<P2> u1[3], P2 f)
+  {
+    const P2 nf = -f;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      {
+        acc_add(acc[c], u0[c], f, nf);
+        acc_add(acc[3 + c], u1[c], f, nf);
+        if (FWD)
+          {
+            if (MU == 0) { acc_add(acc[6 + c], u0[c], f, nf); acc_add(acc[9 + c], u1[c], f, nf); }
+            if (MU == 1) { acc_isub(acc[6 + c], u1[c], f, nf); acc_isub(acc[9 + c], u0[c], f, nf); }
+            if (MU == 2) { acc_sub(acc[6 + c], u1[c], f, nf); acc_add(acc[9 + c], u0[c], f, nf); }
+            if (MU == 3) { acc_isub(acc[6 + c], u0[c], f, nf); acc_iadd(acc[9 + c], u1[c], f, nf); }
+          }
+        else
+          {
+            if (MU == 0) { acc_sub(acc[6 + c], u0[c], f, nf); acc_sub(acc[9 + c], u1[c], f, nf); }
+            if (MU == 1) { acc_iadd(acc[6 + c], u1[c], f, nf); acc_iadd(acc[9 + c], u0[c], f, nf); }
+            if (MU == 2) { acc_add(acc[6 + c], u1[c], f, nf); acc_sub(acc[9 + c], u0[c], f, nf); }
+            if (MU == 3) { acc_iadd(acc[6 + c], u0[c], f, nf); acc_isub(acc[9 + c], u1[c], f, nf); }
+          }
+      }
+  }
+
+  // neighbour of the second site from that of the first: half a volume of
+  // e/o indices away, modulo Vh
+  __device__ __forceinline__ int partner(int n, int hv) { return (n >= hv) ? n - hv : n + hv; }
+
+  template <int MU, bool FWD, int P, int LF>
+  __device__ __forceinline__ void hop_dir2(const Lattice& g, const Site& s, int p, int ieo, int hv,
+                                           const SpinorT<P>& in, const LinkT<LF>& U, float anis, C<P2> acc[12])
+  {
+    const float fmu = (MU > 0) ? anis : 1.0f;
+    bool wa;
+    const int na = FWD ? nbr_up<MU>(g, s, wa) : nbr_dw<MU>(g, s, wa);
+    const int nb = partner(na, hv);
+    // the second site (time t + T/2) crosses the boundary forward from t = T-1;
+    // backward it never does (t + T/2 >= 1)
+    const bool wb = (MU == 0) && FWD && (s.t == (g.T >> 1) - 1);
+    C<P2> sp[12], h0[3], h1[3], u0[3], u1[3], L[9];
+    {
+      C<float> a[12], b[12];
+      float sa, sb;
+      in.load_raw(na, a, sa);
+      in.load_raw(nb, b, sb);
+#pragma unroll
+      for (int c = 0; c < 12; c++) sp[c] = zip(a[c], b[c]);
+      const float fbc = fmu * float(g.bc_t);
+      const float k = LinkT<LF>::kUnit;
+      const P2 f = p2((wa ? fbc : fmu) * sa * k, (wb ? fbc : fmu) * sb * k);
+      project<MU, FWD>(sp, h0, h1);
+      if (FWD) load_link2(U, p, MU, ieo, ieo + hv, L);
+      else load_link2(U, 1 - p, MU, na, nb, L);
+      link_mul2<FWD>(L, h0, u0);
+      link_mul2<FWD>(L, h1, u1);
+      reconstruct2<MU, FWD>(acc, u0, u1, f);
+    }
+  }
+
+  constexpr int HOP2_THREADS = 128;
+
+  // registers capped for 3 resident blocks per SM
+  template <int P, int LF, class Epi, class Fin>
+  __global__ void __launch_bounds__(HOP2_THREADS, 3)
+    hop2_kernel(Lattice g, int par_out, int npar, SpinorT<P> in_e, SpinorT<P> in_o, LinkT<LF> U, const OpParams* prm,
+                Epi epi, Reducer red, Fin fin, const int* __restrict__ stop)
+  {
+    if (stop && *stop) return;
+    const int hv = (int)(g.Vh >> 1);
+    const int idx = blockIdx.x * HOP2_THREADS + threadIdx.x;
+    int p = par_out, ieo = idx;
+    if (npar == 2)
+      {
+        p = (idx >= hv) ? 1 : 0;
+        ieo = idx - (p ? hv : 0);
+      }
+    const bool active = (idx < npar * hv);
+    double part = 0.0;
+    if (active)
+      {
+        C<P2> acc[12];
+#pragma unroll
+        for (int c = 0; c < 12; c++) acc[c] = {p2(0.f, 0.f), p2(0.f, 0.f)};
+        const float anis = float(prm->anis);
+        const Site s = eo_site(g, p, ieo);
+        const SpinorT<P> in = p ? in_e : in_o;
+        hop_dir2<0, true, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        hop_dir2<0, false, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        hop_dir2<1, true, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        hop_dir2<1, false, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        hop_dir2<2, true, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        hop_dir2<2, false, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        hop_dir2<3, true, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        hop_dir2<3, false, P, LF>(g, s, p, ieo, hv, in, U, anis, acc);
+        C<float> a[12], b[12];
+#pragma unroll
+        for (int c = 0; c < 12; c++)
+          {
+            a[c] = {acc[c].re.v.x, acc[c].im.v.x};
+            b[c] = {acc[c].re.v.y, acc[c].im.v.y};
+          }
+        part = epi(p, ieo, a);
+        part += epi(p, ieo + hv, b);
+      }
+    if (Epi::kReduce) grid_reduce<HOP2_THREADS>(part, red, fin);
   }
 
   // ------------------------------------------------------- BLAS kernels

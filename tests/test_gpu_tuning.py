@@ -1,0 +1,67 @@
+"""Every launch shape and link format of the low-precision hops gives the same
+solution: mixed-precision solves under each tuning choice must reach the
+target true residual, agree with the FP64 solve and take about as many
+iterations.  Shapes 3 and 4 select the two-sites-per-thread packed-FP32
+kernel, which pairs the sites t and t+T/2 (T a multiple of 4; other T fall
+back to the one-site kernel)."""
+import numpy as np
+import pytest
+
+from nissa_b200 import Lattice, TmError
+from nissa_b200 import workload as wl
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+KAPPA, MU = 0.1610, 0.005
+
+
+def _solve_all(lat, src, prec, settings):
+    out = []
+    for key, val in settings:
+        lat.set_tuning(key, val)
+        sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-20, precision=prec)
+        out.append((key, val, sol, st))
+    return out
+
+
+@pytest.mark.parametrize("T,L", [(16, 8), (8, 4), (6, 4)])
+@pytest.mark.parametrize("precision", ["single", "half"])
+def test_hop_shapes_agree(cuda_device, T, L, precision):
+    conf = wl.gauge_conf(T, L, 0.35, seed=31)
+    src = wl.random_spinor(T * L ** 3 // 2, 7)
+    key = "hop_cfg_" + precision
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        ref, st0 = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-22)
+        links = [0, 1] if precision == "single" else [0]
+        for ls in links:
+            lat.set_tuning("links_single", ls)
+            for key_, val, sol, st in _solve_all(lat, src, precision, [(key, v) for v in range(5)]):
+                assert st["true_rel_res2"] < 1e-20, (ls, val, st)
+                assert rel(sol, ref) < 1e-8, (ls, val)
+                assert st["iterations"] <= 1.1 * st0["iterations"] + 5, (ls, val, st["iterations"], st0["iterations"])
+
+
+def test_full_lattice_packed(cuda_device):
+    """The full-lattice operator (both parities in one launch) under the packed kernel."""
+    T, L = 8, 4
+    conf = wl.gauge_conf(T, L, 0.35, seed=32)
+    src = wl.random_spinor(T * L ** 3, 8)
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        ref, _ = lat.inv_tmQ2_cg(KAPPA, MU, src, 100000, 1e-22)
+        for prec in ("single", "half"):
+            for v in (0, 3, 4):
+                lat.set_tuning("hop_cfg_" + prec, v)
+                sol, st = lat.inv_tmQ2_cg(KAPPA, MU, src, 100000, 1e-20, precision=prec)
+                assert rel(sol, ref) < 1e-8, (prec, v)
+
+
+def test_shape_range_checked(cuda_device):
+    with Lattice(4, 4) as lat:
+        with pytest.raises(TmError):
+            lat.set_tuning("hop_cfg_double", 3)
+        with pytest.raises(TmError):
+            lat.set_tuning("hop_cfg_single", 5)
+        lat.set_tuning("hop_cfg_half", 4)
