@@ -7,14 +7,17 @@ preconditioned CG, the reference's inv_tmD_cg_eoprec): 32^3 x 64 lattice,
 gauge links U = exp(i eps H) with eps = 0.35 (seeded), antiperiodic time,
 kappa = 0.1610, mu = 0.005, point sources at the origin cycling over the 12
 spin-colour columns, stopped at |r|/|b| <= 1e-10 (squared residue 1e-20), in
-mixed precision: FP32 inner CG with 12-real links and FP64 reliable updates.
+mixed precision: FP16 inner CG (half spinors with a per-site FP32 scale,
+16-bit fixed-point 12-real links) with FP64 reliable updates, the final true
+residual checked in FP64 (--precision single|double selects the others).
 
 Printed JSON line (rank 0): value = solves/s with the inputs resident in HBM
 (device timing, CUDA events, max over ranks); e2e = the same through the C
 ABI with host (pinned) buffers, host<->device copies inside the timed region;
-roofline = the inner solver's hopping kernel (FP32, 12-real links) timed alone
-with CUDA events, L2 flushed between launches; fp64 = the plain FP64 GPU CG on
-the same solves and the FP64 e/o Dslash bandwidth; cpu_baseline = the
+roofline = the inner solver's hopping kernel (hop + inverse diagonal, the first
+half of K) timed alone with CUDA events, L2 flushed between launches; fp64 = the
+plain FP64 GPU CG on the same solves and the FP64 e/o Dslash bandwidth;
+variants = the other inner precisions on the same solves; cpu_baseline = the
 reference's own OpenMP CG (oracle/_ref) on a bounded sample of the same solve.
 
 N > 1 GPUs run independent replicas (one gauge copy per GPU, each rank solving
@@ -36,11 +39,18 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(name="tm e/o CG solve, 32^3x64, mixed FP32-inner/FP64-reliable, |r|/|b|<=1e-10",
+WORKLOAD = dict(name="tm e/o CG solve, 32^3x64, mixed %s-inner/FP64-reliable, |r|/|b|<=1e-10",
                 T=64, L=32, eps=0.35, seed=1, kappa=0.1610, mu=0.005, residue=1e-20, bc_t=-1.0)
+PREC_NAME = {"double": "FP64", "single": "FP32", "half": "FP16"}
+PREC_DTYPE = {"double": "f64", "single": "f32 inner / f64 reliable updates",
+              "half": "f16 storage, f32 arithmetic inner / f64 reliable updates"}
 METRIC = "CG solves/s & Dslash HBM GB/s, 32³×64 mixed vs FP64 @1e-10; p50/p99 serve"
 UNIT = "solves/s"
 CPU_SAMPLE_ITERS = 20
+HOP_KERNEL = {"half": "hop_kernel<FP16 spinors, 16-bit 12-real links> + inverse diagonal (first half of K)",
+              "single": "hop_kernel<FP32 spinors, FP32 12-real links> + inverse diagonal (first half of K)"}
+# DRAM bytes of one launch of that kernel on this workload, from ncu
+HOP_TRAFFIC = {"half": 298.2e6}
 
 
 def log(*a):
@@ -154,7 +164,7 @@ def run_reference_arm(args):
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                       "data": "synthetic (seeded gauge recipe)",
-                      "config": {"workload": W["name"].replace("mixed FP32-inner/FP64-reliable", "FP64 CPU"),
+                      "config": {"workload": W["name"].split(", mixed")[0] + ", FP64 on the host cores, |r|/|b|<=1e-10",
                                  "T": T, "L": L, "kappa": W["kappa"], "mu": W["mu"], "eps": W["eps"],
                                  "residue": W["residue"]},
                       "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
@@ -195,7 +205,9 @@ def run_ours(args):
     cols = [column((rank * args.steps + k) % 12) for k in range(ncol)]
     sol = torch.empty((V, 4, 3, 2), dtype=torch.float64, device=dev)
 
-    def solve(k, precision="single", src=None, out=None):
+    prec = args.precision
+
+    def solve(k, precision=prec, src=None, out=None):
         s = cols[k % ncol] if src is None else src
         return lat.inv_tmD_cg_eoprec(kappa, mu, s, 100000, residue, precision=precision,
                                      out=sol if out is None else out)[1]
@@ -256,14 +268,28 @@ def run_ours(args):
     f0 = time.perf_counter()
     for k in range(fp64_steps):
         fp64_stats.append(solve(k, precision="double", out=ref))
-        solve(k, precision="single", out=sol)
+        solve(k, out=sol)
         errs.append(float(torch.linalg.norm(sol - ref) / torch.linalg.norm(ref)))
     fp64_sec = statistics.mean(s["seconds"] for s in fp64_stats)
     mixed_sec = statistics.mean(s["seconds"] for s in stats)
 
+    # --- the other inner precisions on the same solves (solver-reported device seconds) -----
+    variants = {}
+    for name, vp, links16 in (("single", "single", 0), ("single_links16", "single", 1), ("half", "half", 0)):
+        if vp == prec and not links16:
+            continue
+        lat.set_tuning("links_single", links16)
+        solve(0, precision=vp)
+        vs = [solve(k, precision=vp) for k in range(2)]
+        variants[name] = {"solves_per_s": 1.0 / statistics.mean(x["seconds"] for x in vs),
+                          "iterations": vs[0]["iterations"], "reliable_updates": vs[0]["reliable_updates"],
+                          "true_rel_res2_max": max(x["true_rel_res2"] for x in vs)}
+    lat.set_tuning("links_single", 0)
+
     # --- roofline: the inner solver's hopping kernel, and the FP64 Dslash -------------------
     peak, peak_kind = peaks()
-    hop_ms, hop_bytes = lat.bench_hop("single", variant=1, nrep=30, flush=True)
+    hop_prec = prec if prec != "double" else "single"
+    hop_ms, hop_bytes = lat.bench_hop(hop_prec, variant=1, nrep=30, flush=True)
     d64_ms, d64_bytes = lat.bench_hop("double", variant=0, nrep=30, flush=True)
     achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
     d64_gbs = d64_bytes / (d64_ms * 1e-3) / 1e9
@@ -290,18 +316,22 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 inner / f64 reliable updates",
+        "dtype": PREC_DTYPE[prec],
         "data": "synthetic (seeded gauge recipe U=exp(i eps H), point sources)",
         "config": {"workload": W["name"], "T": T, "L": L, "kappa": kappa, "mu": mu, "eps": W["eps"],
                    "residue_sq": residue, "sources": "12 point spin-colour columns at the origin, cycled",
-                   "l2": "working set (links 0.4 GB FP32 + spinors) larger than the 126 MB L2",
+                   "inner_precision": prec,
+                   "l2": "working set (links 0.2-0.4 GB + spinors) larger than the 126 MB L2",
                    "parallelism": "replicas" if ws > 1 else "1 GPU"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_per, "d2h_bytes_per_step": bytes_per,
                 "steps": e2e_steps},
-        "roofline": {"bound": "hbm", "kernel": "hop_kernel<FP32, 12-real links> + inverse diagonal (CG first half)",
+        "roofline": {"bound": "hbm", "kernel": HOP_KERNEL[hop_prec],
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "ms_per_launch": hop_ms,
-                     "alg_bytes_per_launch": hop_bytes},
+                     "peak_kind": peak_kind, "traffic": HOP_TRAFFIC.get(hop_prec),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
+                                       "kernel on this workload (profiles/)",
+                     "ms_per_launch": hop_ms, "alg_bytes_per_launch": hop_bytes},
+        "variants": variants,
         "fp64": {"solves_per_s": 1.0 / fp64_sec, "iterations": fp64_stats[0]["iterations"],
                  "mixed_speedup_vs_fp64": fp64_sec / mixed_sec,
                  "dslash_gbs": d64_gbs, "dslash_frac": d64_gbs / peak, "dslash_ms": d64_ms},
@@ -440,7 +470,10 @@ def main():
     ap.add_argument("--requests", type=int, default=0, help="serve: number of requests")
     ap.add_argument("--serve-precision", default="single", choices=["double", "single", "half"])
     ap.add_argument("--cgm-precision", default="single", choices=["single", "half"])
+    ap.add_argument("--precision", default="half", choices=["double", "single", "half"],
+                    help="inner precision of the headline solve")
     args = ap.parse_args()
+    WORKLOAD["name"] = WORKLOAD["name"] % PREC_NAME[args.precision]
     if args.lattice:
         T, L = (int(x) for x in args.lattice.split(","))
         WORKLOAD.update(T=T, L=L, name=WORKLOAD["name"].replace("32^3x64", "%d^3x%d" % (L, T)))
@@ -462,7 +495,7 @@ def main():
 # FP64 CG iterations of one full solve of this workload (measured on the GPU's
 # plain FP64 CG, which matches the reference's iteration count; printed by each
 # run of this script under "fp64.iterations").
-FP64_ITERS = 1000
+FP64_ITERS = 99
 
 if __name__ == "__main__":
     main()
