@@ -201,8 +201,9 @@ def run_ours(args):
         s[0, (k // 3) % 4, k % 3, 0] = 1.0
         return s
 
+    from nissa_b200 import replicas
     ncol = min(12, args.steps)
-    cols = [column((rank * args.steps + k) % 12) for k in range(ncol)]
+    cols = [column(c) for c in replicas.rank_columns(rank, args.steps)[:ncol]]
     sol = torch.empty((V, 4, 3, 2), dtype=torch.float64, device=dev)
 
     prec = args.precision
@@ -233,12 +234,8 @@ def run_ours(args):
         e1.record()
         barrier()
     launches = lat.launch_count - l0
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = ws * args.steps / (ms_max * 1e-3)
+    ms_max = replicas.max_over_ranks(e0.elapsed_time(e1))
+    value = replicas.whole_job_rate(args.steps, ms_max, ws)
     clocks = clk.summary()
 
     # --- e2e: same solves through the C ABI with pinned host buffers -----------------------
@@ -253,11 +250,7 @@ def run_ours(args):
     for k in range(e2e_steps):
         solve(k, src=host_src[k % ncol], out=host_sol)
     barrier()
-    e2e_s = time.perf_counter() - h0
-    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = ws * e2e_steps / float(t.item())
+    e2e_value = replicas.whole_job_rate(e2e_steps, replicas.max_over_ranks((time.perf_counter() - h0) * 1e3), ws)
     bytes_per = V * 24 * 8
 
     # --- plain FP64 GPU CG on the same solves, and the accuracy of the mixed solutions -------
@@ -416,6 +409,78 @@ def run_cgm(args):
           flush=True)
 
 
+BATCH_WORKLOAD = dict(name="48-RHS batched e/o CG, 24^3x48: 12 spin-colour-diluted Z2 sources x mu in "
+                           "{+0.003, -0.003, +0.006, -0.006}, mixed %s-inner/FP64-reliable, |r|/|b|<=1e-10",
+                      T=48, L=24, eps=0.35, seed=3, kappa=0.1610, mus=[0.003, -0.003, 0.006, -0.006], residue=1e-20,
+                      bc_t=-1.0)
+
+
+def run_batched(args):
+    """The batched workload: the 48 right-hand sides solved in one batched
+    solve (one launch per operator step for all of them, CUDA graphs,
+    autotuned kernel shapes) against the same 48 solved one at a time with
+    the same precision; reports right-hand sides per second and the largest
+    difference between a batched and an alone solution (an extra line, not
+    the headline)."""
+    import torch
+    from nissa_b200 import Lattice, tune
+    from nissa_b200 import workload as wl
+    W = BATCH_WORKLOAD
+    prec = args.precision
+    T, L = W["T"], W["L"]
+    if args.lattice:
+        T, L = (int(x) for x in args.lattice.split(","))
+    dev = "cuda:0"
+    conf = wl.gauge_conf(T, L, W["eps"], W["seed"], device=dev)
+    lat = Lattice(T, L, bc_t=W["bc_t"])
+    lat.upload_conf(conf)
+    srcs, mus = [], []
+    for k in range(12):
+        z = torch.from_numpy(wl.z2_source(T, L, 100 + k, spin=k // 3, col=k % 3)).to(dev)
+        for mu in W["mus"]:
+            srcs.append(z)
+            mus.append(mu)
+    n = len(srcs)
+    tuned_b = tune.autotune(lat, prec, nrhs=n)
+    tuned_1 = tune.autotune(lat, prec, nrhs=1)
+    outs = [torch.empty_like(srcs[0]) for _ in range(n)]
+    alone = [torch.empty_like(srcs[0]) for _ in range(n)]
+    kappa, res = W["kappa"], W["residue"]
+
+    def batched():
+        return lat.inv_tmD_cg_eoprec_batched(kappa, mus, srcs, 100000, res, precision=prec, out=outs)[1]
+
+    batched()  # capture the graphs
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st_b = batched()
+        e1.record()
+        torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    lat.inv_tmD_cg_eoprec(kappa, mus[0], srcs[0], 100000, res, precision=prec, out=alone[0])
+    torch.cuda.synchronize()
+    e0.record()
+    st_1 = [lat.inv_tmD_cg_eoprec(kappa, mus[i], srcs[i], 100000, res, precision=prec, out=alone[i])[1]
+            for i in range(n)]
+    e1.record()
+    torch.cuda.synchronize()
+    ms_1 = e0.elapsed_time(e1)
+    diff = max(float(torch.linalg.norm(outs[i] - alone[i]) / torch.linalg.norm(alone[i])) for i in range(n))
+    print(json.dumps({"workload": (W["name"] % PREC_NAME[prec]).replace("24^3x48", "%d^3x%d" % (L, T)),
+                      "rhs": n, "precision": prec,
+                      "batched": {"rhs_per_s": n / (ms_b * 1e-3), "ms": ms_b,
+                                  "iterations_max": max(s["iterations"] for s in st_b),
+                                  "true_rel_res2_max": max(s["true_rel_res2"] for s in st_b)},
+                      "one_at_a_time": {"rhs_per_s": n / (ms_1 * 1e-3), "ms": ms_1,
+                                        "iterations_max": max(s["iterations"] for s in st_1),
+                                        "true_rel_res2_max": max(s["true_rel_res2"] for s in st_1)},
+                      "batched_speedup": ms_1 / ms_b,
+                      "max_rel_diff_batched_vs_alone": diff,
+                      "tuning": {"batched": tuned_b, "single": tuned_1}, "clocks": clk.summary()}), flush=True)
+
+
 SERVE_WORKLOAD = dict(volumes={"8^3x16": (16, 8), "16^3x32": (32, 16), "32^3x64": (64, 32)},
                       probs=[0.5, 0.35, 0.15], eps=0.35, seed=1, rate=20.0, requests=200, nslots=16)
 
@@ -464,8 +529,9 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
     ap.add_argument("--hop-cfg", type=int, default=-1, help="hopping-kernel launch shape for --kernel-only (tuning)")
-    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve"],
-                    help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop (extra reports)")
+    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve", "batched"],
+                    help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop; "
+                         "batched: 48 right-hand sides batched vs one at a time (extra reports)")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--requests", type=int, default=0, help="serve: number of requests")
     ap.add_argument("--serve-precision", default="single", choices=["double", "single", "half"])
@@ -485,6 +551,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args)
+        return
+    if args.workload == "batched":
+        run_batched(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)

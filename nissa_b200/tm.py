@@ -147,6 +147,7 @@ class Lattice:
         self.V = T * self.LX * self.LY * self.LZ
         self.Vh = self.V // 2
         self.bc_t = bc_t
+        self.device = device
         h = ctypes.c_void_p()
         st = self.lib.tms_create4(ctypes.byref(h), T, self.LX, self.LY, self.LZ, float(bc_t), device)
         if st != 0:

@@ -65,3 +65,22 @@ def test_shape_range_checked(cuda_device):
         with pytest.raises(TmError):
             lat.set_tuning("hop_cfg_single", 5)
         lat.set_tuning("hop_cfg_half", 4)
+
+
+def test_autotune_on_device(cuda_device, tmp_path):
+    """The autotuner times real kernels, applies a valid choice and reuses its cache;
+    a solve under the tuned choice still reaches the target."""
+    from nissa_b200 import tune
+    T, L = 8, 4
+    conf = wl.gauge_conf(T, L, 0.35, seed=33)
+    src = wl.random_spinor(T * L ** 3 // 2, 9)
+    cache = str(tmp_path / "tune.json")
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        r = tune.autotune(lat, "half", cache=cache)
+        assert not r["cached"] and r["settings"]["hop_cfg_half"] in tune.HOP_SHAPES["half"]
+        rb = tune.autotune(lat, "half", nrhs=8, cache=cache)
+        assert rb["settings"]["mrhs_per_thread"] in tune.MRHS_CHOICES
+        assert tune.autotune(lat, "half", cache=cache)["cached"]
+        sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-20, precision="half")
+        assert st["true_rel_res2"] < 1e-20
