@@ -481,6 +481,92 @@ def run_batched(args):
                       "tuning": {"batched": tuned_b, "single": tuned_1}, "clocks": clk.summary()}), flush=True)
 
 
+def run_configs(args):
+    """The two configurations below the headline volume, each with the
+    reference's own CPU code timed on the same inputs (rank 0 host cores):
+    (1) 8^3x16 plain FP64 e/o CG, kappa 0.16, mu 0.01, eps 0.4, point source,
+    |r|/|b| <= 1e-12; (2) 16^3x32 mixed FP32-inner (12-real links) / FP64
+    reliable updates, kappa 0.161, mu 0.005, eps 0.35, the 12 point columns
+    one at a time, |r|/|b| <= 1e-10, each solution compared with the FP64 GPU
+    solve (itself within 1e-9 of the reference's).  An extra line, not the
+    headline."""
+    import torch
+    from nissa_b200 import Lattice
+    from nissa_b200 import workload as wl
+    dev = "cuda:0"
+    threads = os.cpu_count() or 1
+    res = {}
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = [fn() for _ in range(n)]
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, out
+
+    def reference_full_solve(conf, T, L, kappa, mu, src, residue):
+        try:
+            import oracle
+            if not oracle.ref_available():
+                return None, None
+            conf_bc = wl.apply_time_bc(conf, T, L, -1.0)
+            sol, rec, _ = oracle.run_ref("cgfull", T, L, {"conf": conf_bc, "in": src}, (T * L ** 3, 4, 3, 2),
+                                         kappa=kappa, mu=mu, niter=100000, residue=residue, threads=threads)
+            return sol, rec.get("seconds_per_rep")
+        except Exception as e:  # the CPU leg is reported, never required
+            log("reference CPU solve unavailable: %s" % e)
+            return None, None
+
+    # (1) 8^3x16 plain FP64 CG
+    T, L = 16, 8
+    conf = wl.gauge_conf(T, L, 0.4, 1)
+    src = wl.point_source(T, L)
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        s_d = torch.from_numpy(src).to(dev)
+        sol = torch.empty_like(s_d)
+        ms, st = timed(lambda: lat.inv_tmD_cg_eoprec(0.16, 0.01, s_d, 100000, 1e-24, out=sol)[1], 5)
+        ref_sol, ref_s = reference_full_solve(conf, T, L, 0.16, 0.01, src, 1e-24)
+        err = None if ref_sol is None else float(np.linalg.norm(sol.cpu().numpy() - ref_sol) / np.linalg.norm(ref_sol))
+        res["8^3x16 FP64 CG, point source, 1e-12"] = {
+            "gpu_ms_per_solve": ms, "iterations": st[-1]["iterations"], "lx_rel_res2": st[-1]["lx_rel_res2"],
+            "reference_cpu_s_per_solve": ref_s, "cpu_threads": threads, "rel_err_vs_reference": err,
+            "speedup_vs_reference_cpu": None if ref_s is None else ref_s / (ms * 1e-3)}
+
+    # (2) 16^3x32 mixed FP32 inner, 12 point columns one at a time
+    T, L = 32, 16
+    conf = wl.gauge_conf(T, L, 0.35, 1, device=dev)
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        cols = [torch.from_numpy(wl.point_source(T, L, spin=k // 3, col=k % 3)).to(dev) for k in range(12)]
+        mixed = [torch.empty_like(cols[0]) for _ in range(12)]
+        fp64 = [torch.empty_like(cols[0]) for _ in range(12)]
+
+        def solve_all(prec, outs):
+            return [lat.inv_tmD_cg_eoprec(0.161, 0.005, cols[k], 100000, 1e-20, precision=prec, out=outs[k])[1]
+                    for k in range(12)]
+        ms_m, st_m = timed(lambda: solve_all("single", mixed), 1)
+        ms_d, st_d = timed(lambda: solve_all("double", fp64), 1)
+        errs = [float(torch.linalg.norm(mixed[k] - fp64[k]) / torch.linalg.norm(fp64[k])) for k in range(12)]
+        ref_sol, ref_s = reference_full_solve(conf, T, L, 0.161, 0.005, cols[0].cpu().numpy(), 1e-20)
+        err_ref = None if ref_sol is None else float(
+            np.linalg.norm(fp64[0].cpu().numpy() - ref_sol) / np.linalg.norm(ref_sol))
+        res["16^3x32 mixed FP32 (12-real links), 12 point columns, 1e-10"] = {
+            "gpu_mixed_ms_per_solve": ms_m / 12, "gpu_fp64_ms_per_solve": ms_d / 12,
+            "mixed_speedup_vs_fp64": ms_d / ms_m,
+            "iterations_mixed": [s["iterations"] for s in st_m[-1]],
+            "iterations_fp64": [s["iterations"] for s in st_d[-1]],
+            "true_rel_res2_max": max(s["true_rel_res2"] for s in st_m[-1]),
+            "mixed_rel_err_vs_fp64_max": max(errs),
+            "reference_cpu_s_per_solve": ref_s, "cpu_threads": threads,
+            "fp64_column0_rel_err_vs_reference": err_ref,
+            "speedup_vs_reference_cpu": None if ref_s is None else ref_s / (ms_m / 12 * 1e-3)}
+    print(json.dumps({"workload": "configurations below the headline volume", "results": res}), flush=True)
+
+
 SERVE_WORKLOAD = dict(volumes={"8^3x16": (16, 8), "16^3x32": (32, 16), "32^3x64": (64, 32)},
                       probs=[0.5, 0.35, 0.15], eps=0.35, seed=1, rate=20.0, requests=200, nslots=16)
 
@@ -529,9 +615,10 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
     ap.add_argument("--hop-cfg", type=int, default=-1, help="hopping-kernel launch shape for --kernel-only (tuning)")
-    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve", "batched"],
+    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve", "batched", "configs"],
                     help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop; "
-                         "batched: 48 right-hand sides batched vs one at a time (extra reports)")
+                         "batched: 48 right-hand sides batched vs one at a time; configs: the 8^3x16 and "
+                         "16^3x32 configurations with the reference's CPU solve (extra reports)")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--requests", type=int, default=0, help="serve: number of requests")
     ap.add_argument("--serve-precision", default="single", choices=["double", "single", "half"])
@@ -554,6 +641,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args)
+        return
+    if args.workload == "configs":
+        run_configs(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)
