@@ -468,6 +468,17 @@ def run_batched(args):
     torch.cuda.synchronize()
     ms_1 = e0.elapsed_time(e1)
     diff = max(float(torch.linalg.norm(outs[i] - alone[i]) / torch.linalg.norm(alone[i])) for i in range(n))
+    # the plain FP64 GPU CG on the first 8 right-hand sides, one at a time
+    n64 = 8
+    ref64 = torch.empty_like(srcs[0])
+    lat.inv_tmD_cg_eoprec(kappa, mus[0], srcs[0], 100000, res, precision="double", out=ref64)
+    torch.cuda.synchronize()
+    e0.record()
+    st_64 = [lat.inv_tmD_cg_eoprec(kappa, mus[i], srcs[i], 100000, res, precision="double", out=ref64)[1]
+             for i in range(n64)]
+    e1.record()
+    torch.cuda.synchronize()
+    ms_64 = e0.elapsed_time(e1) / n64
     print(json.dumps({"workload": (W["name"] % PREC_NAME[prec]).replace("24^3x48", "%d^3x%d" % (L, T)),
                       "rhs": n, "precision": prec,
                       "batched": {"rhs_per_s": n / (ms_b * 1e-3), "ms": ms_b,
@@ -476,7 +487,10 @@ def run_batched(args):
                       "one_at_a_time": {"rhs_per_s": n / (ms_1 * 1e-3), "ms": ms_1,
                                         "iterations_max": max(s["iterations"] for s in st_1),
                                         "true_rel_res2_max": max(s["true_rel_res2"] for s in st_1)},
+                      "fp64_one_at_a_time": {"rhs_per_s": 1e3 / ms_64, "ms_per_rhs": ms_64, "rhs_timed": n64,
+                                             "iterations_max": max(s["iterations"] for s in st_64)},
                       "batched_speedup": ms_1 / ms_b,
+                      "batched_mixed_speedup_vs_fp64": ms_64 * n / ms_b,
                       "max_rel_diff_batched_vs_alone": diff,
                       "tuning": {"batched": tuned_b, "single": tuned_1}, "clocks": clk.summary()}), flush=True)
 

@@ -100,6 +100,7 @@ struct tms_ctx
   static constexpr int kGraphs = 8;
   cudaGraphExec_t graph[kGraphs] = {};
   int graph_iters = 8;
+  int batch_iters = 0;  // CG iterations per batch-session graph block (0: by batch size)
   uint64_t graph_nodes[kGraphs] = {};
 
   // tuning (tms_set_tuning): hopping-kernel launch shape per precision, the
