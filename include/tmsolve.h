@@ -36,7 +36,8 @@ typedef enum
   TMS_ERR_TIMEOUT = 5,
   TMS_ERR_CUDA = 6,
   TMS_ERR_NO_CONF = 7,
-  TMS_ERR_INVALID_SOURCE = 8 /* reference: CRASH("invalid norm") */
+  TMS_ERR_INVALID_SOURCE = 8, /* reference: CRASH("invalid norm") */
+  TMS_ERR_IO = 9              /* a file could not be opened, read, written or parsed */
 } tms_status;
 
 typedef enum
@@ -175,6 +176,25 @@ tms_status tms_batch_step(tms_batch *batch, int *finished, int *nfinished);
 /* returns the solve's status (TMS_OK, TMS_ERR_NOT_CONVERGED, TMS_ERR_NAN) */
 tms_status tms_batch_collect(tms_batch *batch, int slot, double *sol_lx, tms_stats *stats);
 tms_status tms_batch_close(tms_batch *batch);
+
+/* ---- gauge configuration files and checks ---- */
+
+/* read_ildg_gauge_conf (io/reader.hpp:75-99, io/ILDG_File.cpp): read the 'ildg-binary-data'
+ * record of an ILDG (LIME) file, big-endian, 32- or 64-bit as its 'ildg-format' record says
+ * (whose lattice sizes must match the context's), reordered to the reference's lx sites and
+ * t,x,y,z directions, into conf_lx (a HOST buffer of V x 72 doubles, whatever the pointer
+ * mode).  No boundary phase is applied (the file holds periodic links). */
+tms_status tms_read_ildg(tms_ctx *ctx, const char *path, double *conf_lx);
+/* The inverse: write conf_lx (host, the reference's lx layout) as an ILDG file with an
+ * 'ildg-format' record and the big-endian 'ildg-binary-data' record; precision 32 or 64. */
+tms_status tms_write_ildg(tms_ctx *ctx, const char *path, const double *conf_lx, int precision);
+/* tms_read_ildg followed by tms_conf_upload(ctx, conf, TMS_LAYOUT_LX, flags). */
+tms_status tms_conf_load_ildg(tms_ctx *ctx, const char *path, int flags);
+/* global_plaquette_lx_conf (operations/su3_paths/plaquette.hpp:25-82) of the uploaded conf,
+ * computed on the device in FP64: the mean of the temporal and spatial averages of
+ * Re tr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+)/3.  with_bc = 0: the periodic links as
+ * stored; 1: with the context's time-boundary sign on the t = T-1 time links. */
+tms_status tms_conf_plaquette(tms_ctx *ctx, int with_bc, double *plaquette);
 
 /* ---- instrumentation (no reference counterpart) ---- */
 

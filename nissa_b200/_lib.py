@@ -33,6 +33,10 @@ SIGNATURES = {
     "tms_geometry_tables": (I, [P, P, P, P, P, P]),
     "tms_conf_upload": (I, [P, P, I, I]),
     "tms_conf_is_su3": (I, [P]),
+    "tms_read_ildg": (I, [P, ctypes.c_char_p, P]),
+    "tms_write_ildg": (I, [P, ctypes.c_char_p, P, I]),
+    "tms_conf_load_ildg": (I, [P, ctypes.c_char_p, I]),
+    "tms_conf_plaquette": (I, [P, I, ctypes.POINTER(D)]),
     "tms_hop_eo": (I, [P, I, P, P, I, D]),
     "tms_tmDee": (I, [P, D, D, P, P]),
     "tms_inv_tmDee": (I, [P, D, D, P, P]),

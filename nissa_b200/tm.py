@@ -23,6 +23,7 @@ lx conf (V, 4, 3, 3, 2), eo conf (2, Vh, 4, 3, 3, 2).
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -203,6 +204,30 @@ class Lattice:
         self._mode(b)
         st = self.lib.tms_conf_upload(self.h, b.ptr, 0 if layout == "lx" else 1, 1 if bc_included else 0)
         self._check(st, "tms_conf_upload")
+
+    def read_ildg(self, path: str) -> np.ndarray:
+        """read_ildg_gauge_conf (io/reader.hpp:75-99): the conf of an ILDG file in the
+        reference's lx layout (V, 4, 3, 3, 2), periodic links as stored."""
+        conf = np.empty((self.V, 4, 3, 3, 2), np.float64)
+        self._check(self.lib.tms_read_ildg(self.h, os.fsencode(path), conf.ctypes.data), "tms_read_ildg")
+        return conf
+
+    def write_ildg(self, path: str, conf, precision: int = 64):
+        """Write an lx conf (V, 4, 3, 3, 2) as an ILDG file (32- or 64-bit big-endian)."""
+        c = np.ascontiguousarray(np.asarray(conf, np.float64).reshape(self.V, 4, 3, 3, 2))
+        self._check(self.lib.tms_write_ildg(self.h, os.fsencode(path), c.ctypes.data, int(precision)),
+                    "tms_write_ildg")
+
+    def load_ildg(self, path: str, bc_included: bool = False):
+        """Read an ILDG file and make it the resident configuration."""
+        self._check(self.lib.tms_conf_load_ildg(self.h, os.fsencode(path), 1 if bc_included else 0),
+                    "tms_conf_load_ildg")
+
+    def plaquette(self, with_bc: bool = False) -> float:
+        """global_plaquette_lx_conf of the resident conf, on the device (FP64)."""
+        p = ctypes.c_double()
+        self._check(self.lib.tms_conf_plaquette(self.h, 1 if with_bc else 0, ctypes.byref(p)), "tms_conf_plaquette")
+        return p.value
 
     @property
     def conf_is_su3(self) -> bool:
