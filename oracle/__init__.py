@@ -83,6 +83,18 @@ def lib():
         L.orc_cgm.argtypes = [P, P, D, I, D, I, P, P, I, P, P, P]
         L.orc_plaquette.restype = D
         L.orc_plaquette.argtypes = [P, P]
+        I64 = ctypes.c_int64
+        L.orc_clover_term.argtypes = [P, P, D, P]
+        L.orc_inv_clover_term.argtypes = [I64, P, D, D, P]
+        L.orc_tmclovDee.argtypes = [I64, P, D, I, D, P, P]
+        L.orc_inv_tmclovDee.argtypes = [I64, P, I, P, P]
+        L.orc_tmclov_kern.argtypes = [P, P, D, I, D, P, P, I, D, P, P]
+        L.orc_tmclov_kern2.argtypes = [P, P, D, I, D, P, P, D, P, P]
+        L.orc_tmclov_cg_eos.restype = I
+        L.orc_tmclov_cg_eos.argtypes = [P, P, D, I, D, P, P, D, I, D, P, P, P, P]
+        L.orc_tmclovQ.argtypes = [P, P, D, I, D, P, D, P, P]
+        L.orc_tmclov_cg_full.restype = I
+        L.orc_tmclov_cg_full.argtypes = [P, P, D, I, D, D, D, I, D, P, P, P]
         _lib = L
     return _lib
 
@@ -200,6 +212,76 @@ class Geom:
         res = ctypes.c_double(0)
         it = lib().orc_cg_full(self._g, _p(conf_lx), kappa, *_anis(anis), mu, int(niter), float(residue), _p(src_lx),
                                _p(sol), ctypes.byref(res))
+        return sol, it, res.value
+
+    # ------------------------------------------------------ twisted clover
+    def clover_term(self, conf_lx, cSW):
+        """clover_term: [V][4][3][3][2] (four leaves, anti-symmetrised, times -cSW/4)."""
+        conf_lx = _c(conf_lx)
+        out = np.empty((self.V, 4, 3, 3, 2))
+        lib().orc_clover_term(self._g, _p(conf_lx), float(cSW), _p(out))
+        return out
+
+    @staticmethod
+    def inv_clover_term(Cl, kappa, mass):
+        """invert_twisted_clover_term: [sites][2][6][6][2]."""
+        Cl = _c(Cl)
+        n = Cl.shape[0]
+        out = np.empty((n, 2, 6, 6, 2))
+        lib().orc_inv_clover_term(n, _p(Cl), float(kappa), float(mass), _p(out))
+        return out
+
+    @staticmethod
+    def tmclovDee(Cl, kappa, dag, mu, inp):
+        Cl, inp = _c(Cl), _c(inp)
+        out = np.empty_like(inp)
+        lib().orc_tmclovDee(Cl.shape[0], _p(Cl), float(kappa), int(dag), float(mu), _p(inp), _p(out))
+        return out
+
+    @staticmethod
+    def inv_tmclovDee(invCl, dag, inp):
+        invCl, inp = _c(invCl), _c(inp)
+        out = np.empty_like(inp)
+        lib().orc_inv_tmclovDee(invCl.shape[0], _p(invCl), int(dag), _p(inp), _p(out))
+        return out
+
+    def tmclov_kern(self, conf_eo, kappa, Cl_odd, invCl_evn, dag, mu, inp, anis=None):
+        conf_eo, Cl_odd, invCl_evn, inp = _c(conf_eo), _c(Cl_odd), _c(invCl_evn), _c(inp)
+        out = np.empty_like(inp)
+        lib().orc_tmclov_kern(self._g, _p(conf_eo), float(kappa), *_anis(anis), _p(Cl_odd), _p(invCl_evn), int(dag),
+                              float(mu), _p(inp), _p(out))
+        return out
+
+    def tmclov_kern2(self, conf_eo, kappa, Cl_odd, invCl_evn, mu, inp, anis=None):
+        conf_eo, Cl_odd, invCl_evn, inp = _c(conf_eo), _c(Cl_odd), _c(invCl_evn), _c(inp)
+        out = np.empty_like(inp)
+        lib().orc_tmclov_kern2(self._g, _p(conf_eo), float(kappa), *_anis(anis), _p(Cl_odd), _p(invCl_evn),
+                               float(mu), _p(inp), _p(out))
+        return out
+
+    def tmclov_cg_eos(self, conf_eo, kappa, Cl_odd, invCl_evn, mu, src, niter, residue, guess=None, anis=None):
+        conf_eo, Cl_odd, invCl_evn, src = _c(conf_eo), _c(Cl_odd), _c(invCl_evn), _c(src)
+        guess = None if guess is None else _c(guess)
+        sol = np.empty((self.Vh, 4, 3, 2))
+        res = ctypes.c_double(0)
+        it = lib().orc_tmclov_cg_eos(self._g, _p(conf_eo), float(kappa), *_anis(anis), _p(Cl_odd), _p(invCl_evn),
+                                     float(mu), int(niter), float(residue), _p(guess), _p(src), _p(sol),
+                                     ctypes.byref(res))
+        return sol, it, res.value
+
+    def tmclovQ(self, conf_lx, kappa, Cl_lx, mu, inp, anis=None):
+        conf_lx, Cl_lx, inp = _c(conf_lx), _c(Cl_lx), _c(inp)
+        out = np.empty_like(inp)
+        lib().orc_tmclovQ(self._g, _p(conf_lx), float(kappa), *_anis(anis), _p(Cl_lx), float(mu), _p(inp), _p(out))
+        return out
+
+    def tmclov_cg_full(self, conf_lx, kappa, cSW, mu, src_lx, niter, residue, anis=None):
+        """inv_tmclovD_cg_eoprec: returns (sol_lx, iterations, lx |g5 Q x - b|^2/|b|^2)."""
+        conf_lx, src_lx = _c(conf_lx), _c(src_lx)
+        sol = np.empty((self.V, 4, 3, 2))
+        res = ctypes.c_double(0)
+        it = lib().orc_tmclov_cg_full(self._g, _p(conf_lx), float(kappa), *_anis(anis), float(cSW), float(mu),
+                                      int(niter), float(residue), _p(src_lx), _p(sol), ctypes.byref(res))
         return sol, it, res.value
 
     def cgm(self, conf_lx, kappa, masses, residues, src, niter, anis=None):

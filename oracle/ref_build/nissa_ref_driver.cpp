@@ -22,6 +22,12 @@
 //        tmQ conf in out kappa mu                apply_tmQ                        (dirac_operator_tmQ_portable.cpp:29-176)
 //        cgm conf in out kappa masses=a,b residues=a,b niter
 //                                                inv_tmclovQ2_cgm with a zero clover term (cgm_invert_tmclovQ2.cpp:10-32)
+//        clover conf out cSW                     clover_term                      (su3_paths/clover_term.hpp:104-112)
+//        invclover conf out cSW kappa mu         invert_twisted_clover_term       (su3_paths/clover_term.hpp:143-262)
+//        clovkern conf in out cSW kappa mu dag   tmclovDkern_eoprec_eos           (dirac_operator_tmclovD_eoprec_portable.cpp:42-68)
+//        clovkern2 conf in out cSW kappa mu      tmclovDkern_eoprec_square_eos    (dirac_operator_tmclovD_eoprec_portable.cpp:70-84)
+//        clovcgfull conf in out cSW kappa mu niter residue
+//                                                inv_tmclovD_cg_eoprec            (cg_invert_tmclovD_eoprec.cpp:55-120)
 //   common keys: anis=<double> (default: none), reps=<n> (timed repetitions, default 1)
 //   cg with sample_iters=N: a bounded sample of the solve.  The reference's CG
 //   runs exactly N iterations (niter=N, unreachable residue) plus its final
@@ -53,6 +59,9 @@
 #include "inverters/twisted_mass/cg_invert_tmD_eoprec.hpp"
 #include "io/reader.hpp"
 #include "operations/su3_paths/plaquette.hpp"
+#include "operations/su3_paths/clover_term.hpp"
+#include "dirac_operators/tmclovD_eoprec/dirac_operator_tmclovD_eoprec.hpp"
+#include "inverters/twisted_clover/cg_invert_tmclovD_eoprec.hpp"
 
 namespace nissa
 {
@@ -219,7 +228,75 @@ int main(int narg, char** arg_v)
       LxField<quad_su3> conf_lx("conf_lx", WITH_HALO);
       fill(conf_lx, read_file(arg("conf"), V * 72), V, 72);
 
-      if (op == "plaq")
+      // the chromo operator reads the conf's edges: a copy allocated with them
+      LxField<quad_su3> conf_edges("conf_edges", WITH_HALO_EDGES);
+      if (op == "clover" || op == "invclover" || op == "clovkern" || op == "clovkern2" || op == "clovcgfull")
+	fill(conf_edges, read_file(arg("conf"), V * 72), V, 72);
+      if (op == "clover" || op == "invclover")
+	{
+	  LxField<clover_term_t> Cl("Cl");
+	  const double t0 = now();
+	  for (int r = 0; r < reps; r++) clover_term(Cl, argd("cSW"), conf_edges);
+	  if (op == "clover")
+	    {
+	      t_per_rep = (now() - t0) / reps;
+	      dump(Cl, arg("out"), V, 72);
+	    }
+	  else
+	    {
+	      LxField<inv_clover_term_t> invCl("invCl");
+	      const double t1 = now();
+	      for (int r = 0; r < reps; r++) invert_twisted_clover_term(invCl, argd("mu"), argd("kappa"), Cl);
+	      t_per_rep = (now() - t1) / reps;
+	      dump(invCl, arg("out"), V, 144);
+	    }
+	}
+      else if (op == "clovcgfull")
+	{
+	  LxField<spincolor> in("in", WITH_HALO);
+	  fill(in, read_file(arg("in"), V * 24), V, 24);
+	  LxField<spincolor> sol("sol", WITH_HALO);
+	  const double t0 = now();
+	  for (int r = 0; r < reps; r++)
+	    inv_tmclovD_cg_eoprec(sol, std::nullopt, conf_edges, argd("kappa"), anis, argd("cSW"), argd("mu"),
+				  (int)argd("niter"), argd("residue"), in);
+	  t_per_rep = (now() - t0) / reps;
+	  dump(sol, arg("out"), V, 24);
+	}
+      else if (op == "clovkern" || op == "clovkern2")
+	{
+	  // the clover fields exactly as inv_tmclovD_cg_eoprec_native builds them
+	  const double kappa = argd("kappa"), mu = argd("mu");
+	  LxField<clover_term_t> Cl_lx("Cl");
+	  clover_term(Cl_lx, argd("cSW"), conf_edges);
+	  LxField<inv_clover_term_t> invCl_lx("invCl");
+	  invert_twisted_clover_term(invCl_lx, mu, kappa, Cl_lx);
+	  OddField<clover_term_t> Cl_odd("Cl_odd");
+	  get_evn_or_odd_part_of_lx_vector(Cl_odd, Cl_lx, ODD_SITES);
+	  EvnField<inv_clover_term_t> invCl_evn("invCl_evn");
+	  get_evn_or_odd_part_of_lx_vector(invCl_evn, invCl_lx, EVEN_SITES);
+	  EoField<quad_su3> conf("conf", WITH_HALO);
+	  split_lx_vector_into_eo_parts(conf, conf_lx);
+	  OddField<spincolor> in("in", WITH_HALO), out("out", WITH_HALO);
+	  fill(in, read_file(arg("in"), Vh * 24), Vh, 24);
+	  const double t0 = now();
+	  if (op == "clovkern")
+	    {
+	      EvnField<spincolor> tmp("tmp", WITH_HALO);
+	      for (int r = 0; r < reps; r++)
+		tmclovDkern_eoprec_eos(out, tmp, conf, kappa, anis, Cl_odd, invCl_evn, argd("dag") != 0, mu, in);
+	    }
+	  else
+	    {
+	      OddField<spincolor> temp1("temp1", WITH_HALO);
+	      EvnField<spincolor> temp2("temp2", WITH_HALO);
+	      for (int r = 0; r < reps; r++)
+		tmclovDkern_eoprec_square_eos(out, temp1, temp2, conf, kappa, anis, Cl_odd, invCl_evn, mu, in);
+	    }
+	  t_per_rep = (now() - t0) / reps;
+	  dump(out, arg("out"), Vh, 24);
+	}
+      else if (op == "plaq")
 	{
 	  const double plaq = global_plaquette_lx_conf(conf_lx);
 	  char buf[64];

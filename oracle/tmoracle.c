@@ -732,3 +732,414 @@ double orc_plaquette(const orc_geom *g, const double *conf_lx)
   free(buf);
   return (p0 + p1) / 2;
 }
+
+/* ================================================================ clover */
+/* The twisted-clover e/o path.  Layouts (float64, AoS):
+ *   clover term   [sites][4][3][3][2]          clover_term_t = su3[4] (new_types/su3.hpp:57-60)
+ *   inverse       [sites][2][2][3][2][3][2]    inv_clover_term_t: per chirality a 6x6
+ *                                              matrix [id][ic][jd][jc] (su3.hpp:31,62) */
+
+/* c = a*b, a*b^+, a^+*b, a^+*b^+ (unsafe_su3_prod_su3 and variants, su3_op.hpp) */
+static void su3_mm(double *c, const double *a, const double *b, int da, int db)
+{
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      {
+        double re = 0, im = 0;
+        for (int k = 0; k < 3; k++)
+          {
+            const double *x = da ? a + 6 * k + 2 * i : a + 6 * i + 2 * k;
+            const double *y = db ? b + 6 * j + 2 * k : b + 6 * k + 2 * j;
+            const double xr = x[0], xi = da ? -x[1] : x[1], yr = y[0], yi = db ? -y[1] : y[1];
+            re += xr * yr - xi * yi;
+            im += xr * yi + xi * yr;
+          }
+        c[6 * i + 2 * j] = re;
+        c[6 * i + 2 * j + 1] = im;
+      }
+}
+
+/* four_leaves_point: measures/gauge/topological_charge.hpp:139-212; planes in the
+ * order of edge_numb (base/init.cpp:705-714): (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) */
+static void four_leaves(const orc_geom *g, const double *conf, int64_t X, double *leaves)
+{
+#define U(site, d) (conf + ((int64_t)(site) * 4 + (d)) * SU3)
+  int munu = 0;
+  for (int mu = 0; mu < 4; mu++)
+    {
+      const int64_t A = g->nup_lx[X * 4 + mu], D = g->ndw_lx[X * 4 + mu];
+      for (int nu = mu + 1; nu < 4; nu++, munu++)
+        {
+          const int64_t B = g->nup_lx[X * 4 + nu], F = g->ndw_lx[X * 4 + nu];
+          const int64_t C = g->nup_lx[D * 4 + nu], E = g->ndw_lx[D * 4 + nu];
+          const int64_t G = g->ndw_lx[A * 4 + nu];
+          double *L = leaves + munu * SU3, t1[SU3], t2[SU3];
+          /* leaf 1 */
+          su3_mm(t1, U(X, mu), U(A, nu), 0, 0);
+          su3_mm(t2, t1, U(B, mu), 0, 1);
+          su3_mm(L, t2, U(X, nu), 0, 1);
+          /* leaf 2 */
+          su3_mm(t1, U(X, nu), U(C, mu), 0, 1);
+          su3_mm(t2, t1, U(D, nu), 0, 1);
+          su3_mm(t1, t2, U(D, mu), 0, 0);
+          for (int k = 0; k < SU3; k++) L[k] += t1[k];
+          /* leaf 3 */
+          su3_mm(t1, U(D, mu), U(E, nu), 1, 1);
+          su3_mm(t2, t1, U(E, mu), 0, 0);
+          su3_mm(t1, t2, U(F, nu), 0, 0);
+          for (int k = 0; k < SU3; k++) L[k] += t1[k];
+          /* leaf 4 */
+          su3_mm(t1, U(F, nu), U(F, mu), 1, 0);
+          su3_mm(t2, t1, U(G, nu), 0, 0);
+          su3_mm(t1, t2, U(X, mu), 0, 1);
+          for (int k = 0; k < SU3; k++) L[k] += t1[k];
+        }
+    }
+#undef U
+}
+
+/* clover_term (operations/su3_paths/clover_term.hpp:104-112): point_chromo_operator
+ * (clover_term.cpp:57-95) times chromo_operator_factor(cSW + 1e-16) /
+ * chromo_operator_factor(-4) (clover_term.hpp:44-84) */
+void orc_clover_term(const orc_geom *g, const double *conf_lx, double cSW, double *Cl)
+{
+  const double factor = (-(cSW + 1e-16) / 4) / (-(-4.0) / 4);
+#pragma omp parallel for
+  for (int64_t X = 0; X < g->V; X++)
+    {
+      double leaves[6 * SU3], P[6][SU3];
+      four_leaves(g, conf_lx, X, leaves);
+      for (int i = 0; i < 6; i++)
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++)
+            {
+              P[i][6 * a + 2 * b] = (leaves[i * SU3 + 6 * a + 2 * b] - leaves[i * SU3 + 6 * b + 2 * a]) / 4;
+              P[i][6 * a + 2 * b + 1] = (leaves[i * SU3 + 6 * a + 2 * b + 1] + leaves[i * SU3 + 6 * b + 2 * a + 1]) / 4;
+            }
+      double *c = Cl + X * 4 * SU3;
+      for (int k = 0; k < SU3; k += 2)
+        {
+          const double Ar = P[3][k] - P[2][k], Ai = P[3][k + 1] - P[2][k + 1];
+          const double Br = P[4][k] + P[1][k], Bi = P[4][k + 1] + P[1][k + 1];
+          const double Cr = P[5][k] - P[0][k], Ci = P[5][k + 1] - P[0][k + 1];
+          const double Dr = P[3][k] + P[2][k], Di = P[3][k + 1] + P[2][k + 1];
+          const double Er = P[4][k] - P[1][k], Ei = P[4][k + 1] - P[1][k + 1];
+          const double Fr = P[5][k] + P[0][k], Fi = P[5][k + 1] + P[0][k + 1];
+          /* Cl0 = iA, Cl1 = B + iC, Cl2 = iD, Cl3 = E + iF */
+          c[0 * SU3 + k] = -Ai * factor;
+          c[0 * SU3 + k + 1] = Ar * factor;
+          c[1 * SU3 + k] = (Br - Ci) * factor;
+          c[1 * SU3 + k + 1] = (Bi + Cr) * factor;
+          c[2 * SU3 + k] = -Di * factor;
+          c[2 * SU3 + k + 1] = Dr * factor;
+          c[3 * SU3 + k] = (Er - Fi) * factor;
+          c[3 * SU3 + k + 1] = (Ei + Fr) * factor;
+        }
+    }
+}
+
+/* the 6x6 twisted clover block of chirality b: z 1 + [[c0, c1^+], [c1, -c0]] with
+ * z = 1/2k + i mass (apply_point_twisted_clover_term_to_halfspincolor, clover_term.hpp:114-141) */
+static void clover_block_z(const double *Cl, int b, double zr, double zi, double M[6][6][2])
+{
+  const double *c0 = Cl + (2 * b) * SU3, *c1 = Cl + (2 * b + 1) * SU3;
+  for (int a = 0; a < 3; a++)
+    for (int e = 0; e < 3; e++)
+      {
+        const double dz = (a == e) ? zr : 0.0, dm = (a == e) ? zi : 0.0;
+        M[a][e][0] = dz + c0[6 * a + 2 * e];
+        M[a][e][1] = dm + c0[6 * a + 2 * e + 1];
+        M[a][3 + e][0] = c1[6 * e + 2 * a];
+        M[a][3 + e][1] = -c1[6 * e + 2 * a + 1];
+        M[3 + a][e][0] = c1[6 * a + 2 * e];
+        M[3 + a][e][1] = c1[6 * a + 2 * e + 1];
+        M[3 + a][3 + e][0] = dz - c0[6 * a + 2 * e];
+        M[3 + a][3 + e][1] = dm - c0[6 * a + 2 * e + 1];
+      }
+}
+
+static void clover_block(const double *Cl, int b, double kappa, double mass, double M[6][6][2])
+{
+  clover_block_z(Cl, b, 1.0 / (2 * kappa), mass, M);
+}
+
+/* invert_twisted_clover_term (clover_term.hpp:143-262): per site and chirality the
+ * inverse of the block with +mass.  The reference solves for each column with a
+ * point CG on the squared block to |r|^2 < 1e-32; the inverse is unique, so this
+ * restatement inverts directly (Gauss-Jordan, partial pivoting) in float64. */
+void orc_inv_clover_term(int64_t nsites, const double *Cl, double kappa, double mass, double *invCl)
+{
+#pragma omp parallel for
+  for (int64_t X = 0; X < nsites; X++)
+    for (int b = 0; b < 2; b++)
+      {
+        double M[6][6][2], I[6][6][2];
+        clover_block(Cl + X * 4 * SU3, b, kappa, mass, M);
+        for (int i = 0; i < 6; i++)
+          for (int j = 0; j < 6; j++) I[i][j][0] = (i == j), I[i][j][1] = 0;
+        for (int col = 0; col < 6; col++)
+          {
+            int piv = col;
+            double best = -1;
+            for (int r = col; r < 6; r++)
+              {
+                const double m = M[r][col][0] * M[r][col][0] + M[r][col][1] * M[r][col][1];
+                if (m > best) best = m, piv = r;
+              }
+            for (int j = 0; j < 6; j++)
+              for (int q = 0; q < 2; q++)
+                {
+                  double t = M[col][j][q]; M[col][j][q] = M[piv][j][q]; M[piv][j][q] = t;
+                  t = I[col][j][q]; I[col][j][q] = I[piv][j][q]; I[piv][j][q] = t;
+                }
+            const double pr = M[col][col][0], pi = M[col][col][1], pn = pr * pr + pi * pi;
+            const double ir = pr / pn, ii = -pi / pn;
+            for (int j = 0; j < 6; j++)
+              {
+                double a = M[col][j][0], c = M[col][j][1];
+                M[col][j][0] = a * ir - c * ii; M[col][j][1] = a * ii + c * ir;
+                a = I[col][j][0]; c = I[col][j][1];
+                I[col][j][0] = a * ir - c * ii; I[col][j][1] = a * ii + c * ir;
+              }
+            for (int r = 0; r < 6; r++)
+              {
+                if (r == col) continue;
+                const double fr = M[r][col][0], fi = M[r][col][1];
+                for (int j = 0; j < 6; j++)
+                  {
+                    M[r][j][0] -= fr * M[col][j][0] - fi * M[col][j][1];
+                    M[r][j][1] -= fr * M[col][j][1] + fi * M[col][j][0];
+                    I[r][j][0] -= fr * I[col][j][0] - fi * I[col][j][1];
+                    I[r][j][1] -= fr * I[col][j][1] + fi * I[col][j][0];
+                  }
+              }
+          }
+        double *o = invCl + X * 144 + b * 72;
+        for (int i = 0; i < 6; i++)
+          for (int j = 0; j < 6; j++)
+            {
+              o[(i * 6 + j) * 2] = I[i][j][0];
+              o[(i * 6 + j) * 2 + 1] = I[i][j][1];
+            }
+      }
+}
+
+/* tmclovDee_or_oo_eos: dirac_operators/tmclovD_eoprec/dirac_operator_tmclovD_eoprec_portable.cpp:18-40 */
+void orc_tmclovDee(int64_t nsites, const double *Cl, double kappa, int dag, double mu, const double *in, double *out)
+{
+  if (dag) mu = -mu;
+#pragma omp parallel for
+  for (int64_t X = 0; X < nsites; X++)
+    for (int b = 0; b < 2; b++)
+      {
+        double M[6][6][2];
+        clover_block(Cl + X * 4 * SU3, b, kappa, b ? -mu : mu, M);
+        const double *i = in + X * SC + b * 12;
+        double *o = out + X * SC + b * 12;
+        for (int r = 0; r < 6; r++)
+          {
+            double re = 0, im = 0;
+            for (int c = 0; c < 6; c++)
+              {
+                re += M[r][c][0] * i[2 * c] - M[r][c][1] * i[2 * c + 1];
+                im += M[r][c][0] * i[2 * c + 1] + M[r][c][1] * i[2 * c];
+              }
+            o[2 * r] = re;
+            o[2 * r + 1] = im;
+          }
+      }
+}
+
+/* inv_tmclovDee_or_oo_eos: dirac_operator_tmclovD_eoprec.hpp:24-44 */
+void orc_inv_tmclovDee(int64_t nsites, const double *invCl, int dag, const double *in, double *out)
+{
+  const int high = dag ? 1 : 0, low = dag ? 0 : 1;
+#pragma omp parallel for
+  for (int64_t X = 0; X < nsites; X++)
+    for (int b = 0; b < 2; b++)
+      {
+        const double *m = invCl + X * 144 + b * 72;
+        const double *i = in + X * SC + b * 12;
+        double *o = out + X * SC + b * 12;
+        for (int r = 0; r < 6; r++)
+          {
+            double re = 0, im = 0;
+            for (int c = 0; c < 6; c++)
+              {
+                if (b == high)
+                  {
+                    const double *e = m + (r * 6 + c) * 2;
+                    re += e[0] * i[2 * c] - e[1] * i[2 * c + 1];
+                    im += e[0] * i[2 * c + 1] + e[1] * i[2 * c];
+                  }
+                else
+                  {
+                    const double *e = m + (c * 6 + r) * 2; /* conj of the transposed element */
+                    re += e[0] * i[2 * c] + e[1] * i[2 * c + 1];
+                    im += e[0] * i[2 * c + 1] - e[1] * i[2 * c];
+                  }
+              }
+            o[2 * r] = re;
+            o[2 * r + 1] = im;
+          }
+        (void)low;
+      }
+}
+
+/* tmclovDkern_eoprec_eos: dirac_operator_tmclovD_eoprec_portable.cpp:42-68 */
+void orc_tmclov_kern(const orc_geom *g, const double *conf_eo, double kappa, int has_anis, double anis,
+                     const double *Cl_odd, const double *invCl_evn, int dag, double mu, const double *in, double *out)
+{
+  const int64_t n = g->Vh * SC;
+  double *te = (double *)malloc(sizeof(double) * n), *to = (double *)malloc(sizeof(double) * n);
+  orc_hop_eo(g, conf_eo, 0, has_anis, anis, in, to);
+  orc_inv_tmclovDee(g->Vh, invCl_evn, dag, to, te);
+  orc_hop_eo(g, conf_eo, 1, has_anis, anis, te, out);
+  orc_tmclovDee(g->Vh, Cl_odd, kappa, dag, mu, in, te);
+#pragma omp parallel for
+  for (int64_t X = 0; X < g->Vh; X++)
+    for (int k = 0; k < 12; k++)
+      {
+        double *o = out + X * SC;
+        const double *t = te + X * SC;
+        o[k] = +t[k] - o[k] * 0.25;
+        o[k + 12] = -t[k + 12] + o[k + 12] * 0.25;
+      }
+  free(te);
+  free(to);
+}
+
+/* tmclovDkern_eoprec_square_eos: dirac_operator_tmclovD_eoprec_portable.cpp:70-84 */
+void orc_tmclov_kern2(const orc_geom *g, const double *conf_eo, double kappa, int has_anis, double anis,
+                      const double *Cl_odd, const double *invCl_evn, double mu, const double *in, double *out)
+{
+  double *t = (double *)malloc(sizeof(double) * g->Vh * SC);
+  orc_tmclov_kern(g, conf_eo, kappa, has_anis, anis, Cl_odd, invCl_evn, 1, mu, in, t);
+  orc_tmclov_kern(g, conf_eo, kappa, has_anis, anis, Cl_odd, invCl_evn, 0, mu, t, out);
+  free(t);
+}
+
+struct clov2_ctx
+{
+  const orc_geom *g;
+  const double *conf_eo, *Cl_odd, *invCl_evn;
+  double kappa;
+  int has_anis;
+  double anis, mu;
+};
+
+static void clov2_op(const void *c, const double *in, double *out)
+{
+  const struct clov2_ctx *k = (const struct clov2_ctx *)c;
+  orc_tmclov_kern2(k->g, k->conf_eo, k->kappa, k->has_anis, k->anis, k->Cl_odd, k->invCl_evn, k->mu, in, out);
+}
+
+/* inv_tmclovDkern_eoprec_square_eos_cg -> _cg_64: inverters/twisted_clover/cg_invert_tmclovD_eoprec.cpp:33-52,
+ * cg_64_invert_tmclovD_eoprec.hpp:11-44 */
+int orc_tmclov_cg_eos(const orc_geom *g, const double *conf_eo, double kappa, int has_anis, double anis,
+                      const double *Cl_odd, const double *invCl_evn, double mu, int niter, double residue,
+                      const double *guess, const double *src, double *sol, double *true_rel_res2)
+{
+  struct clov2_ctx k = {g, conf_eo, Cl_odd, invCl_evn, kappa, has_anis, anis, mu};
+  return cg_invert(g->Vh, clov2_op, &k, niter, residue, guess, src, sol, true_rel_res2);
+}
+
+/* apply_tmclovQ: dirac_operators/tmclovQ/dirac_operator_tmclovQ.cpp:15-170 = apply_tmQ plus
+ * gamma5 times the chromo operator (unsafe_apply_point_chromo_operator_to_spincolor,
+ * clover_term.hpp:14-30) */
+void orc_tmclovQ(const orc_geom *g, const double *conf_lx, double kappa, int has_anis, double anis,
+                 const double *Cl_lx, double mu, const double *in, double *out)
+{
+  orc_tmQ(g, conf_lx, kappa, has_anis, anis, mu, in, out);
+#pragma omp parallel for
+  for (int64_t X = 0; X < g->V; X++)
+    for (int b = 0; b < 2; b++)
+      {
+        double M[6][6][2];
+        clover_block_z(Cl_lx + X * 4 * SU3, b, 0.0, 0.0, M); /* the chromo operator block alone */
+        const double *i = in + X * SC + b * 12;
+        double *o = out + X * SC + b * 12;
+        const double sg = b ? -1.0 : 1.0;
+        for (int r = 0; r < 6; r++)
+          {
+            double re = 0, im = 0;
+            for (int c = 0; c < 6; c++)
+              {
+                const double mr = M[r][c][0], mi = M[r][c][1];
+                re += mr * i[2 * c] - mi * i[2 * c + 1];
+                im += mr * i[2 * c + 1] + mi * i[2 * c];
+              }
+            o[2 * r] += sg * re;
+            o[2 * r + 1] += sg * im;
+          }
+      }
+}
+
+/* inv_tmclovD_cg_eoprec_native + the residual check of inv_tmclovD_cg_eoprec:
+ * inverters/twisted_clover/cg_invert_tmclovD_eoprec.cpp:55-120, :135-220.
+ * *lx_rel_res2 = |g5 Q_clov sol - src|^2/|src|^2 */
+int orc_tmclov_cg_full(const orc_geom *g, const double *conf_lx, double kappa, int has_anis, double anis, double cSW,
+                       double mass, int niter, double residue, const double *src_lx, double *sol_lx,
+                       double *lx_rel_res2)
+{
+  const int64_t V = g->V, Vh = g->Vh, n = Vh * SC;
+  double *Cl_lx = (double *)malloc(sizeof(double) * V * 4 * SU3);
+  double *Cl_eo = (double *)malloc(sizeof(double) * V * 4 * SU3);
+  double *invCl_lx = (double *)malloc(sizeof(double) * V * 144);
+  double *invCl_eo = (double *)malloc(sizeof(double) * V * 144);
+  orc_clover_term(g, conf_lx, cSW, Cl_lx);
+  orc_inv_clover_term(V, Cl_lx, kappa, mass, invCl_lx);
+  orc_split_lx_to_eo(g, Cl_lx, 4 * SU3, Cl_eo);
+  orc_split_lx_to_eo(g, invCl_lx, 144, invCl_eo);
+  const double *Cl_odd = Cl_eo + Vh * 4 * SU3, *invCl_evn = invCl_eo;
+  double *conf_eo = (double *)malloc(sizeof(double) * V * QSU3);
+  double *src_eo = (double *)malloc(sizeof(double) * 2 * n), *sol_eo = (double *)malloc(sizeof(double) * 2 * n);
+  double *evnTemp = (double *)malloc(sizeof(double) * n), *varphi = (double *)malloc(sizeof(double) * n);
+  double *oddTemp = (double *)malloc(sizeof(double) * n);
+  orc_split_lx_to_eo(g, conf_lx, QSU3, conf_eo);
+  orc_split_lx_to_eo(g, src_lx, SC, src_eo);
+  const double *src_e = src_eo, *src_o = src_eo + n;
+  /* Eq. 8a */
+  orc_inv_tmclovDee(Vh, invCl_evn, 0, src_e, evnTemp);
+  /* Eq. 8b (inv_tmD_cg_eoprec_prepare_source, twisted_mass/cg_invert_tmD_eoprec.cpp:37-58) */
+  orc_hop_eo(g, conf_eo, 1, has_anis, anis, evnTemp, varphi);
+#pragma omp parallel for
+  for (int64_t X = 0; X < Vh; X++)
+    for (int k = 0; k < 12; k++)
+      {
+        double *v = varphi + X * SC;
+        const double *s = src_o + X * SC;
+        v[k] = +s[k] + v[k] * 0.5;
+        v[k + 12] = -s[k + 12] - v[k + 12] * 0.5;
+      }
+  /* Eq. 9 */
+  double cg_res;
+  const int it = orc_tmclov_cg_eos(g, conf_eo, kappa, has_anis, anis, Cl_odd, invCl_evn, mass, niter, residue, NULL,
+                                   varphi, oddTemp, &cg_res);
+  /* Eq. 10 */
+  double *sol_e = sol_eo, *sol_o = sol_eo + n;
+  orc_tmclov_kern(g, conf_eo, kappa, has_anis, anis, Cl_odd, invCl_evn, 1, mass, oddTemp, sol_o);
+  /* Eq. 11 */
+  orc_hop_eo(g, conf_eo, 0, has_anis, anis, sol_o, evnTemp);
+#pragma omp parallel for
+  for (int64_t i = 0; i < n; i++) evnTemp[i] = src_e[i] + evnTemp[i] * 0.5;
+  orc_inv_tmclovDee(Vh, invCl_evn, 0, evnTemp, sol_e);
+  orc_paste_eo_to_lx(g, sol_eo, SC, sol_lx);
+  if (lx_rel_res2)
+    {
+      double *rv = (double *)malloc(sizeof(double) * V * SC);
+      orc_tmclovQ(g, conf_lx, kappa, has_anis, anis, Cl_lx, mass, sol_lx, rv);
+#pragma omp parallel for
+      for (int64_t X = 0; X < V; X++)
+        for (int k = 0; k < SC; k++)
+          {
+            const double gv = (k < 12 ? 1 : -1) * rv[X * SC + k];
+            rv[X * SC + k] = gv - src_lx[X * SC + k];
+          }
+      *lx_rel_res2 = scalar_prod(V, rv, rv) / scalar_prod(V, src_lx, src_lx);
+      free(rv);
+    }
+  free(Cl_lx); free(Cl_eo); free(invCl_lx); free(invCl_eo);
+  free(conf_eo); free(src_eo); free(sol_eo); free(evnTemp); free(varphi); free(oddTemp);
+  return it;
+}

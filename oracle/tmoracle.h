@@ -58,6 +58,24 @@ int orc_cgm(const orc_geom *g, const double *conf_lx, double kappa, int has_anis
             const double *masses, const double *residues, int niter, const double *src, double *sols,
             double *true_rel_res2);
 
+/* twisted clover (clover term [sites][4][3][3][2], inverse [sites][2][6][6][2]) */
+void orc_clover_term(const orc_geom *g, const double *conf_lx, double cSW, double *Cl_lx);
+void orc_inv_clover_term(int64_t nsites, const double *Cl, double kappa, double mass, double *invCl);
+void orc_tmclovDee(int64_t nsites, const double *Cl, double kappa, int dag, double mu, const double *in, double *out);
+void orc_inv_tmclovDee(int64_t nsites, const double *invCl, int dag, const double *in, double *out);
+void orc_tmclov_kern(const orc_geom *g, const double *conf_eo, double kappa, int has_anis, double anis,
+                     const double *Cl_odd, const double *invCl_evn, int dag, double mu, const double *in, double *out);
+void orc_tmclov_kern2(const orc_geom *g, const double *conf_eo, double kappa, int has_anis, double anis,
+                      const double *Cl_odd, const double *invCl_evn, double mu, const double *in, double *out);
+int orc_tmclov_cg_eos(const orc_geom *g, const double *conf_eo, double kappa, int has_anis, double anis,
+                      const double *Cl_odd, const double *invCl_evn, double mu, int niter, double residue,
+                      const double *guess, const double *src, double *sol, double *true_rel_res2);
+void orc_tmclovQ(const orc_geom *g, const double *conf_lx, double kappa, int has_anis, double anis,
+                 const double *Cl_lx, double mu, const double *in, double *out);
+int orc_tmclov_cg_full(const orc_geom *g, const double *conf_lx, double kappa, int has_anis, double anis, double cSW,
+                       double mass, int niter, double residue, const double *src_lx, double *sol_lx,
+                       double *lx_rel_res2);
+
 double orc_plaquette(const orc_geom *g, const double *conf_lx);
 double orc_norm2(int64_t n, const double *v);
 

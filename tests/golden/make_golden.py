@@ -7,6 +7,8 @@ inputs.
 Fixtures:
   ref_T4L4.npz      4^4 lattice: every operator on the path and the CG / full
                     solve / multi-shift solves, inputs included.
+  ref_T4L4_clover.npz  4^4 twisted clover: clover term, inverse, Schur operator,
+                    its square and the full e/o solve.
   ref_T16L8_cg.npz  8^3x16 lattice, the plain FP64 CG workload (kappa=0.16,
                     mu=0.01, eps=0.4, point source, |r|/|b| <= 1e-12): the
                     conf is regenerated from its seed, the fixture keeps the
@@ -86,6 +88,34 @@ def make_cg(path):
     print("wrote", path, "iters", iters_from(so, "Total cg iterations"), "plaq", prec["plaquette"])
 
 
+def make_clover(path):
+    """Twisted clover on 4^4: the clover term, its twisted inverse (every 8th
+    site), the Schur operator for both dagger flags, its square, and the full
+    e/o solve inv_tmclovD_cg_eoprec (|r|/|b| <= 1e-12) with its iteration count."""
+    T, L = 4, 4
+    V, Vh = T * L ** 3, T * L ** 3 // 2
+    kappa, mu, cSW = 0.135, 0.03, 1.6
+    conf = wl.gauge_conf(T, L, 0.4, seed=5)
+    conf_bc = wl.apply_time_bc(conf, T, L, -1.0)
+    rng = np.random.Generator(np.random.Philox(13))
+    x = rng.standard_normal((Vh, 4, 3, 2))
+    src = rng.standard_normal((V, 4, 3, 2))
+    sh = (Vh, 4, 3, 2)
+    out = {}
+    out["clover"], _, _ = oracle.run_ref("clover", T, L, {"conf": conf_bc}, (V, 4, 3, 3, 2), cSW=cSW)
+    inv, _, _ = oracle.run_ref("invclover", T, L, {"conf": conf_bc}, (V, 2, 6, 6, 2), cSW=cSW, kappa=kappa, mu=mu)
+    out["invclover_every8"] = inv[::8]
+    for dag in (0, 1):
+        out["kern_dag%d" % dag], _, _ = oracle.run_ref("clovkern", T, L, {"conf": conf_bc, "in": x}, sh, cSW=cSW,
+                                                       kappa=kappa, mu=mu, dag=dag)
+    out["kern2"], _, _ = oracle.run_ref("clovkern2", T, L, {"conf": conf_bc, "in": x}, sh, cSW=cSW, kappa=kappa, mu=mu)
+    out["cgfull"], _, so = oracle.run_ref("clovcgfull", T, L, {"conf": conf_bc, "in": src}, (V, 4, 3, 2), cSW=cSW,
+                                          kappa=kappa, mu=mu, niter=10000, residue=1e-24)
+    out["cgfull_iters"] = np.array(iters_from(so, "Total cg iterations"))
+    np.savez_compressed(path, T=T, L=L, bc_t=-1.0, kappa=kappa, mu=mu, cSW=cSW, conf=conf, x=x, src=src, **out)
+    print("wrote", path, {k: (v.shape if hasattr(v, "shape") else v) for k, v in out.items()})
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -93,3 +123,4 @@ if __name__ == "__main__":
     oracle.build_ref(a.ref)
     make_small(os.path.join(HERE, "ref_T4L4.npz"))
     make_cg(os.path.join(HERE, "ref_T16L8_cg.npz"))
+    make_clover(os.path.join(HERE, "ref_T4L4_clover.npz"))

@@ -115,3 +115,33 @@ def test_unit_conf_plaquette_and_free_hop():
     a = geo.hop(ceo, 0, x)
     b = geo.hop(ceo, 0, 2 * x)
     assert rel(b, 2 * a) < 1e-15
+
+
+@pytest.fixture(scope="module")
+def golden_clover():
+    return dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_T4L4_clover.npz")))
+
+
+def test_clover_oracle_matches_reference(golden_clover):
+    """Twisted clover: clover term, twisted inverse, Schur operator (both dagger
+    flags), its square and the full e/o solve against the reference's own outputs."""
+    g = golden_clover
+    T, L = int(g["T"]), int(g["L"])
+    kappa, mu, cSW = float(g["kappa"]), float(g["mu"]), float(g["cSW"])
+    geo = oracle.Geom(T, L)
+    V, Vh = geo.V, geo.Vh
+    conf_bc = wl.apply_time_bc(g["conf"], T, L, float(g["bc_t"]))
+    Cl = geo.clover_term(conf_bc, cSW)
+    assert rel(Cl, g["clover"]) < 1e-14
+    inv = geo.inv_clover_term(Cl, kappa, mu)
+    assert rel(inv[::8], g["invclover_every8"]) < 1e-14
+    ceo = geo.split(conf_bc)
+    Cl_eo = geo.split(Cl.reshape(V, -1)).reshape(2, Vh, 4, 3, 3, 2)
+    inv_eo = geo.split(inv.reshape(V, -1)).reshape(2, Vh, 2, 6, 6, 2)
+    for dag in (0, 1):
+        assert rel(geo.tmclov_kern(ceo, kappa, Cl_eo[1], inv_eo[0], dag, mu, g["x"]), g["kern_dag%d" % dag]) < 1e-14
+    assert rel(geo.tmclov_kern2(ceo, kappa, Cl_eo[1], inv_eo[0], mu, g["x"]), g["kern2"]) < 1e-14
+    sol, it, lxres = geo.tmclov_cg_full(conf_bc, kappa, cSW, mu, g["src"], 10000, 1e-24)
+    assert it == int(g["cgfull_iters"])
+    assert rel(sol, g["cgfull"]) < 1e-12
+    assert lxres < 1e-23
