@@ -177,6 +177,44 @@ tms_status tms_batch_step(tms_batch *batch, int *finished, int *nfinished);
 tms_status tms_batch_collect(tms_batch *batch, int slot, double *sol_lx, tms_stats *stats);
 tms_status tms_batch_close(tms_batch *batch);
 
+/* ---- twisted clover: the reference's tmclov e/o path ---- */
+
+/* clover_term (operations/su3_paths/clover_term.hpp:104-112; chromo_operator clover_term.cpp:57-95,
+ * four_leaves_point measures/gauge/topological_charge.hpp:139-212): compute on the device, in FP64,
+ * the clover term of the uploaded conf as the reference's operators see it (time-boundary sign
+ * on the t = T-1 time links) times -(cSW + 1e-16)/4, and keep it until the next conf upload.
+ * The operators below use it; the twisted inverse on even sites (invert_twisted_clover_term,
+ * clover_term.hpp:143-262) is computed for each (kappa, mu) on first use and kept. */
+tms_status tms_clover_term(tms_ctx *ctx, double cSW);
+/* the kept clover term in the reference's lx layout: V x [4][3][3][re,im] (LxField<clover_term_t>) */
+tms_status tms_clover_get(tms_ctx *ctx, double *cl_lx);
+/* tmclovDee_or_oo_eos (dirac_operators/tmclovD_eoprec/dirac_operator_tmclovD_eoprec_portable.cpp:18-40)
+ * on the Vh sites of parity par */
+tms_status tms_tmclovDee(tms_ctx *ctx, int par, double kappa, double mu, int dag, const double *in, double *out);
+/* inv_tmclovDee_or_oo_eos (dirac_operator_tmclovD_eoprec.hpp:24-44) on the even sites */
+tms_status tms_inv_tmclovDee(tms_ctx *ctx, double kappa, double mu, int dag, const double *in, double *out);
+/* tmclovDkern_eoprec_eos (dirac_operator_tmclovD_eoprec_portable.cpp:42-68): odd -> odd */
+tms_status tms_tmclovDkern_eoprec(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu, int dag,
+                                  const double *in, double *out);
+/* tmclovDkern_eoprec_square_eos (dirac_operator_tmclovD_eoprec_portable.cpp:70-84): K(false) K(true) */
+tms_status tms_tmclovDkern_eoprec_square(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu,
+                                         const double *in, double *out);
+/* apply_tmclovQ (dirac_operators/tmclovQ/dirac_operator_tmclovQ.cpp:15-170): lx -> lx */
+tms_status tms_apply_tmclovQ(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu, const double *in,
+                             double *out);
+/* inv_tmclovDkern_eoprec_square_eos_cg (inverters/twisted_clover/cg_invert_tmclovD_eoprec.cpp:33-52,
+ * cg_64_invert_tmclovD_eoprec.hpp:11-44): CG on K(false)K(true), odd sites, with the kept clover term */
+tms_status tms_cg_tmclov_eoprec_square(tms_ctx *ctx, double *sol, const double *guess, const double *src,
+                                       double kappa, int has_anis, double anis, double mu, int niter, double residue,
+                                       int precision, tms_stats *stats);
+/* inv_tmclovD_cg_eoprec (inverters/twisted_clover/cg_invert_tmclovD_eoprec.cpp:55-220): full solve in
+ * lx via e/o preconditioning (Eq. 8-11 with the clover diagonal), computing the clover term for cSW
+ * when it differs from the kept one; stats->lx_rel_res2 is the reference's final check
+ * |g5 Q_clov sol - src|^2/|src|^2 */
+tms_status tms_cg_tmclov_eoprec(tms_ctx *ctx, double *sol_lx, const double *src_lx, double kappa, int has_anis,
+                                double anis, double cSW, double mu, int niter, double residue, int precision,
+                                tms_stats *stats);
+
 /* ---- gauge configuration files and checks ---- */
 
 /* read_ildg_gauge_conf (io/reader.hpp:75-99, io/ILDG_File.cpp): read the 'ildg-binary-data'

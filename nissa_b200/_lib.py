@@ -33,6 +33,15 @@ SIGNATURES = {
     "tms_geometry_tables": (I, [P, P, P, P, P, P]),
     "tms_conf_upload": (I, [P, P, I, I]),
     "tms_conf_is_su3": (I, [P]),
+    "tms_clover_term": (I, [P, D]),
+    "tms_clover_get": (I, [P, P]),
+    "tms_tmclovDee": (I, [P, I, D, D, I, P, P]),
+    "tms_inv_tmclovDee": (I, [P, D, D, I, P, P]),
+    "tms_tmclovDkern_eoprec": (I, [P, D, I, D, D, I, P, P]),
+    "tms_tmclovDkern_eoprec_square": (I, [P, D, I, D, D, P, P]),
+    "tms_apply_tmclovQ": (I, [P, D, I, D, D, P, P]),
+    "tms_cg_tmclov_eoprec_square": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
+    "tms_cg_tmclov_eoprec": (I, [P, P, P, D, I, D, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_read_ildg": (I, [P, ctypes.c_char_p, P]),
     "tms_write_ildg": (I, [P, ctypes.c_char_p, P, I]),
     "tms_conf_load_ildg": (I, [P, ctypes.c_char_p, I]),

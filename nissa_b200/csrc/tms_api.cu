@@ -156,6 +156,10 @@ tms_status tms_destroy(tms_ctx* ctx)
   fr(ctx->xlo32.n);
   fr(ctx->lx_of_eo);
   fr(ctx->U64);
+  fr(ctx->cl64);
+  fr(ctx->cl32);
+  fr(ctx->icl64);
+  fr(ctx->icl32);
   fr(ctx->U32r);
   fr(ctx->U32f);
   fr(ctx->U16r);
@@ -236,6 +240,7 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
   CU(cudaGetLastError());
   ctx->su3 = (dev < 1e-10);
   ctx->conf_loaded = true;
+  ctx->clov_ok = ctx->icl_ok = false; // a clover term belongs to the conf it was computed from
   return TMS_OK;
 }
 

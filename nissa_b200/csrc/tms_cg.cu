@@ -132,6 +132,61 @@ namespace
     }
   };
 
+  // ClovOp: K_clov(dag=false) K_clov(dag=true) on odd sites
+  // (inv_tmclovDkern_eoprec_square_eos_cg), on the e/o fields of EoOp
+  struct ClovOp
+  {
+    static constexpr int slot0 = 8;
+    static constexpr int nlo = 6;
+    static int stride(tms_ctx* c) { return c->g.stride; }
+    static int nsites(tms_ctx* c) { return (int)c->g.Vh; }
+    static Field* hi(tms_ctx* c) { return c->f64; }
+    static Field* lo(tms_ctx* c) { return c->lo; }
+    static int& lo_prec(tms_ctx* c) { return c->lo_prec; }
+    static Field& xlo(tms_ctx* c) { return c->xlo32; }
+
+    // r = b - K(false)K(true) x in FP64; returns |r|^2 (uses hi 4, 5, 6)
+    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr)
+    {
+      Field &t1 = ctx->f64[4], &te = ctx->f64[5], &s = ctx->f64[6];
+      auto U = links64(ctx);
+      clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), x, te, t1, 1, ctx->prm);
+      clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), t1, te, s, 0, ctx->prm);
+      const int n = nsites(ctx);
+      ++ctx->launches;
+      residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+        n, view<PREC_F64>(b), view<PREC_F64>(s), view<PREC_F64>(r), reducer(ctx));
+      CU(cudaGetLastError());
+      *rr = read_result(ctx);
+      return TMS_OK;
+    }
+
+    // `iters` CG iterations in precision P (x in PX): v 1 r, 2 p, 3 t1, 4 te.
+    // (p, K(false)K(true) p) = |K(true) p|^2 is reduced in the second launch.
+    template <int P, int PX, int LF>
+    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters)
+    {
+      const Field &r = v[1], &p = v[2], &t1 = v[3], &te = v[4];
+      const int* stop = &c->st->stop;
+      const OpParams* prm = c->prm;
+      const ClovT<P> cl = clov<P>(c);
+      for (int it = 0; it < iters; it++)
+        {
+          EpiInvClov<P> a1{{view<P>(te), view<P>(te)}, cl, 1};
+          launch_hop<P, LF>(c, s, 0, 1, p, p, U, prm, a1, NoFin{}, stop);
+          EpiClovKern<P, true> b1{{view<P>(t1), view<P>(t1)}, {view<P>(p), view<P>(p)}, cl, prm, 1};
+          launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b1, FinAlpha{c->st}, stop);
+          EpiInvClov<P> a2{{view<P>(te), view<P>(te)}, cl, 0};
+          launch_hop<P, LF>(c, s, 0, 1, t1, t1, U, prm, a2, NoFin{}, stop);
+          EpiClovKernCgUpdate<P, PX> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), cl, prm, c->st};
+          launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+          const int n = nsites(c);
+          ++c->launches;
+          xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s>>>(n, view<P>(r), view<P>(p), c->st, stop);
+        }
+    }
+  };
+
   // capture a block of iterations once per (slot, fields); replayed every launch
   template <class Rec>
   tms_status capture(tms_ctx* ctx, int slot, const Rec& rec)
@@ -260,6 +315,9 @@ namespace
         TRY(drop_graph(ctx, Op::slot0 + 1));
         TRY(drop_graph(ctx, Op::slot0 + 2));
         if (Op::slot0 == LxOp::slot0) TRY(drop_graph(ctx, 7));
+        // the twisted-mass and twisted-clover e/o solvers share the inner fields
+        if (Op::slot0 == EoOp::slot0 || Op::slot0 == ClovOp::slot0)
+          for (int k : {EoOp::slot0 + 1, EoOp::slot0 + 2, ClovOp::slot0 + 1, ClovOp::slot0 + 2}) TRY(drop_graph(ctx, k));
         for (int i = 0; i < Op::nlo; i++) TRY(alloc_field(ctx, lo[i], P, Op::stride(ctx)));
         Op::lo_prec(ctx) = P;
       }
@@ -583,6 +641,97 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
   return st;
 }
 
+
+// ------------------------------------------------------------ twisted clover
+tms_status tms_cg_tmclov_eoprec_square(tms_ctx* ctx, double* sol, const double* guess, const double* src, double kappa,
+                                       int has_anis, double anis, double mu, int niter, double residue, int precision,
+                                       tms_stats* stats)
+{
+  TRY(check_clover(ctx));
+  if (!sol || !src || niter <= 0 || !(residue > 0)) return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
+  TRY(set_params(ctx, kappa, mu, has_anis, anis));
+  TRY(ensure_clover_inverse(ctx, kappa, mu));
+  Field* f = ctx->f64;
+  TRY(spinor_in(ctx, src, nullptr, ctx->g.Vh, f[0]));
+  if (guess) TRY(spinor_in(ctx, guess, nullptr, ctx->g.Vh, f[1]));
+  const tms_status st = cg_dispatch<ClovOp>(ctx, precision, niter, residue, guess != nullptr, stats);
+  if (st == TMS_OK || st == TMS_ERR_NOT_CONVERGED) TRY(spinor_out(ctx, f[1], nullptr, ctx->g.Vh, sol, true));
+  TRY(finish(ctx));
+  return st;
+}
+
+tms_status tms_cg_tmclov_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, double kappa, int has_anis,
+                                double anis, double cSW, double mu, int niter, double residue, int precision,
+                                tms_stats* stats)
+{
+  TRY(check_conf(ctx));
+  if (!sol_lx || !src_lx || niter <= 0 || !(residue > 0)) return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
+  // clover_term(Cl, cSW, conf) and invert_twisted_clover_term(invCl, mu, kappa, Cl) of the call
+  // (cg_invert_tmclovD_eoprec.cpp:72-76), kept across calls with the same conf and parameters
+  if (!ctx->clov_ok || ctx->clov_csw != cSW) TRY(tms_clover_term(ctx, cSW));
+  TRY(set_params(ctx, kappa, mu, has_anis, anis));
+  TRY(ensure_clover_inverse(ctx, kappa, mu));
+  Field* f = ctx->f64;
+  for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
+  Field *eta = ctx->ex, *psi = ctx->ex + 2; // [0] even, [1] odd
+  for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
+  const int64_t Vh = ctx->g.Vh;
+  const int n = (int)Vh;
+  const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
+  auto V = [&](const Field& x) { return view<PREC_F64>(x); };
+  auto U = links64(ctx);
+  const double* src = src_lx;
+  if (ctx->ptr_mode == TMS_PTR_HOST)
+    {
+      TRY(ensure_stage(ctx, bytes));
+      CU(cudaMemcpyAsync(ctx->stage, src_lx, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      src = ctx->stage;
+    }
+  ++ctx->launches;
+  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(eta[0]));
+  ++ctx->launches;
+  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
+  // Eq. (8a): te = T_ee^-1 eta_e ; Eq. (8b): varphi = g5 (eta_o + hop(te)/2) -> f0  (:84-90)
+  inv_clov_apply(ctx, eta[0], f[5], 0);
+  EpiSrcPrep<PREC_F64> sp{{V(f[0]), V(f[0])}, {V(eta[1]), V(eta[1])}};
+  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
+  CU(cudaGetLastError());
+  // Eq. (9)
+  const tms_status st = cg_dispatch<ClovOp>(ctx, precision, niter, residue, false, stats);
+  if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+  // Eq. (10): psi_o = K(dag) x ; Eq. (11): psi_e = T_ee^-1 (eta_e + hop(psi_o)/2)  (:97-107)
+  clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), f[1], f[5], psi[1], 1, ctx->prm);
+  EpiClovReco<PREC_F64> rc{{V(psi[0]), V(psi[0])}, {V(eta[0]), V(eta[0])}, clov64(ctx)};
+  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
+  CU(cudaGetLastError());
+  double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sol_lx;
+  ++ctx->launches;
+  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, d);
+  ++ctx->launches;
+  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, d);
+  CU(cudaGetLastError());
+  if (ctx->ptr_mode == TMS_PTR_HOST) CU(cudaMemcpyAsync(sol_lx, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  // the residual check of inv_tmclovD_cg_eoprec (:140-175): |g5 Q_clov sol - src|^2 / |src|^2
+  if (stats)
+    {
+      tmclovQ_op(ctx, psi[0], psi[1], f[2], f[3], ctx->prm);
+      double num = 0, den = 0;
+      for (int par = 0; par < 2; par++)
+        {
+          ++ctx->launches;
+          g5_residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, V(f[2 + par]), V(eta[par]),
+                                                                                       reducer(ctx));
+          CU(cudaGetLastError());
+          num += read_result(ctx);
+          double e2;
+          TRY(norm2<PREC_F64>(ctx, eta[par], &e2));
+          den += e2;
+        }
+      stats->lx_rel_res2 = num / den;
+    }
+  TRY(finish(ctx));
+  return st;
+}
 
 tms_status tms_cg_tmQ2(tms_ctx* ctx, double* sol_lx, const double* guess_lx, const double* src_lx, double kappa,
                        int has_anis, double anis, double m, int niter, double residue, int precision,

@@ -5,6 +5,7 @@
 #include "tmsolve.h"
 #include "tms_kernels.cuh"
 #include "tms_pipe.cuh"
+#include "tms_clover.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -95,9 +96,19 @@ struct tms_ctx
   void* cgm_ps = nullptr;
   int cgm_prec = -1, cgm_nshift = 0;
 
+  // twisted clover (tms_clover_term): the clover term of both parities and
+  // the twisted inverse on even sites for (icl_kappa, icl_mu)
+  bool clov_ok = false, icl_ok = false;
+  double clov_csw = 0.0, icl_kappa = 0.0, icl_mu = 0.0;
+  double2* cl64 = nullptr;  // [par][36][Vh]
+  float2* cl32 = nullptr;
+  double2* icl64 = nullptr; // [2 chiralities][6][6][Vh], even sites
+  float2* icl32 = nullptr;
+
   // CUDA graphs of one iteration block: 0-2 e/o CG (FP64, FP32, FP16),
-  // 3-5 full-lattice CG (FP64, FP32, FP16), 6-7 CGM (FP64, FP32)
-  static constexpr int kGraphs = 8;
+  // 3-5 full-lattice CG (FP64, FP32, FP16), 6-7 CGM (FP64, FP32),
+  // 8-10 e/o twisted-clover CG (FP64, FP32, FP16)
+  static constexpr int kGraphs = 11;
   cudaGraphExec_t graph[kGraphs] = {};
   int graph_iters = 8;
   int batch_iters = 0;  // CG iterations per batch-session graph block (0: by batch size)
@@ -543,6 +554,47 @@ namespace tms_int
     launch_hop<P, LF>(c, c->stream, 1, 1, te, te, U, prm, eb);
   }
 
+
+  // ------------------------------------------------- twisted clover helpers
+  inline ClovT<PREC_F64> clov64(tms_ctx* c) { return ClovT<PREC_F64>{c->cl64, c->icl64, (int)c->g.Vh}; }
+  inline ClovT<PREC_F32> clov32(tms_ctx* c) { return ClovT<PREC_F32>{c->cl32, c->icl32, (int)c->g.Vh}; }
+  inline ClovT<PREC_F16> clov16(tms_ctx* c) { return ClovT<PREC_F16>{c->cl32, c->icl32, (int)c->g.Vh}; }
+  template <int P> ClovT<P> clov(tms_ctx* c);
+  template <> inline ClovT<PREC_F64> clov<PREC_F64>(tms_ctx* c) { return clov64(c); }
+  template <> inline ClovT<PREC_F32> clov<PREC_F32>(tms_ctx* c) { return clov32(c); }
+  template <> inline ClovT<PREC_F16> clov<PREC_F16>(tms_ctx* c) { return clov16(c); }
+
+  inline tms_status check_clover(tms_ctx* ctx)
+  {
+    TRY(check_conf(ctx));
+    if (!ctx->clov_ok) return fail(ctx, TMS_ERR_NO_CONF, "no clover term: call tms_clover_term after the conf upload");
+    return TMS_OK;
+  }
+
+  // the twisted inverse on even sites for (kappa, mu), recomputed when they change (tms_clover.cu)
+  tms_status ensure_clover_inverse(tms_ctx* ctx, double kappa, double mu);
+  // out = T_ee^-1(dag) in on even sites, FP64 (tms_clover.cu)
+  void inv_clov_apply(tms_ctx* c, const Field& in, const Field& out, int dag);
+
+  // out = K_clov(dag) in  (odd -> odd), te is the even temporary
+  template <int P, int LF>
+  void clov_kern_op(tms_ctx* c, const LinkT<LF>& U, const ClovT<P>& cl, const Field& in, const Field& te,
+                    const Field& out, int dag, const OpParams* prm)
+  {
+    EpiInvClov<P> ea{{view<P>(te), view<P>(te)}, cl, dag};
+    launch_hop<P, LF>(c, c->stream, 0, 1, in, in, U, prm, ea);
+    EpiClovKern<P, false> eb{{view<P>(out), view<P>(out)}, {view<P>(in), view<P>(in)}, cl, prm, dag};
+    launch_hop<P, LF>(c, c->stream, 1, 1, te, te, U, prm, eb);
+  }
+
+  // Q_clov on the full lattice, FP64: (in_e, in_o) -> (out_e, out_o)
+  inline void tmclovQ_op(tms_ctx* c, const Field& in_e, const Field& in_o, const Field& out_e, const Field& out_o,
+                         const OpParams* prm)
+  {
+    EpiTmClovQ<PREC_F64> e{{view<PREC_F64>(out_e), view<PREC_F64>(out_o)},
+                           {view<PREC_F64>(in_e), view<PREC_F64>(in_o)}, clov64(c), prm};
+    launch_hop<PREC_F64, LINK_F64_18>(c, c->stream, 0, 2, in_e, in_o, links64(c), prm, e);
+  }
 
   inline tms_status push_state(tms_ctx* ctx)
   {

@@ -394,6 +394,74 @@ class Lattice:
     def batch_session(self, nslots: int, precision: str = "single", anis=None) -> BatchSession:
         return BatchSession(self, nslots, precision, anis)
 
+    # ------------------------------------------------------ twisted clover
+    def clover_term(self, cSW: float):
+        """clover_term(Cl, cSW, conf): computed and kept on the device for the resident conf."""
+        self._check(self.lib.tms_clover_term(self.h, float(cSW)), "tms_clover_term")
+
+    def clover_get(self) -> np.ndarray:
+        """The kept clover term in the reference's lx layout (V, 4, 3, 3, 2), on the host."""
+        out = np.empty((self.V, 4, 3, 3, 2), np.float64)
+        b = _Buf(out, out.shape, out=True)
+        self._mode(b)
+        self._check(self.lib.tms_clover_get(self.h, b.ptr), "tms_clover_get")
+        return out
+
+    def tmclovDee_or_oo_eos(self, par, kappa, mu, dag, inp, out=None):
+        return self._unary(self.lib.tms_tmclovDee, lambda i, o: (int(par), kappa, mu, int(bool(dag)), i, o), inp,
+                           (self.Vh, 4, 3, 2), out)
+
+    def inv_tmclovDee_or_oo_eos(self, kappa, mu, dag, inp, out=None):
+        return self._unary(self.lib.tms_inv_tmclovDee, lambda i, o: (kappa, mu, int(bool(dag)), i, o), inp,
+                           (self.Vh, 4, 3, 2), out)
+
+    def tmclovDkern_eoprec_eos(self, kappa, mu, dag, inp, anis=None, out=None):
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_tmclovDkern_eoprec, lambda i, o: (kappa, a[0], a[1], mu, int(bool(dag)), i, o),
+                           inp, (self.Vh, 4, 3, 2), out)
+
+    def tmclovDkern_eoprec_square_eos(self, kappa, mu, inp, anis=None, out=None):
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_tmclovDkern_eoprec_square, lambda i, o: (kappa, a[0], a[1], mu, i, o), inp,
+                           (self.Vh, 4, 3, 2), out)
+
+    def apply_tmclovQ(self, kappa, mu, inp, anis=None, out=None):
+        a = self._anis(anis)
+        return self._unary(self.lib.tms_apply_tmclovQ, lambda i, o: (kappa, a[0], a[1], mu, i, o), inp,
+                           (self.V, 4, 3, 2), out)
+
+    def inv_tmclovDkern_eoprec_square_eos_cg(self, kappa, mu, source, niter, residue, guess=None, anis=None,
+                                             precision="double", out=None, raise_on_error=True):
+        """Solve K_clov(false)K_clov(true) sol = source on odd sites (kept clover term).  Returns (sol, stats)."""
+        shape = (self.Vh, 4, 3, 2)
+        s, g = _Buf(source, shape), _Buf(guess, shape)
+        sol = self._new_out(source, shape) if out is None else out
+        o = _Buf(sol, shape, out=True)
+        self._mode(s, g, o)
+        stats = _lib.Stats()
+        a = self._anis(anis)
+        st = self.lib.tms_cg_tmclov_eoprec_square(self.h, o.ptr, g.ptr, s.ptr, kappa, a[0], a[1], mu, int(niter),
+                                                  float(residue), PRECISION[precision], ctypes.byref(stats))
+        if raise_on_error:
+            self._check(st, "inv_tmclovDkern_eoprec_square_eos_cg", stats.as_dict(), sol)
+        return sol, stats.as_dict()
+
+    def inv_tmclovD_cg_eoprec(self, kappa, cSW, mu, source_lx, niter, residue, anis=None, precision="double",
+                              out=None, raise_on_error=True):
+        """Full solve of the twisted-clover operator (lx spinors) via e/o preconditioning.  Returns (sol, stats)."""
+        shape = (self.V, 4, 3, 2)
+        s = _Buf(source_lx, shape)
+        sol = self._new_out(source_lx, shape) if out is None else out
+        o = _Buf(sol, shape, out=True)
+        self._mode(s, o)
+        stats = _lib.Stats()
+        a = self._anis(anis)
+        st = self.lib.tms_cg_tmclov_eoprec(self.h, o.ptr, s.ptr, kappa, a[0], a[1], float(cSW), mu, int(niter),
+                                           float(residue), PRECISION[precision], ctypes.byref(stats))
+        if raise_on_error:
+            self._check(st, "inv_tmclovD_cg_eoprec", stats.as_dict(), sol)
+        return sol, stats.as_dict()
+
     def inv_tmD_cg_eoprec(self, kappa, mu, source_lx, niter, residue, anis=None, precision="double", out=None,
                           raise_on_error=True):
         """Full solve D_tm sol = source (lx spinors) via e/o preconditioning.  Returns (sol, stats)."""
