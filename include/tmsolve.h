@@ -215,6 +215,24 @@ tms_status tms_cg_tmclov_eoprec(tms_ctx *ctx, double *sol_lx, const double *src_
                                 double anis, double cSW, double mu, int niter, double residue, int precision,
                                 tms_stats *stats);
 
+/* ---- caller-side steps around a propagator solve ---- */
+
+/* safe_dirac_prod_spincolor with P- (r = 0) or P+ (r = 1), the twisted-basis rotation of
+ * projects/ib/prop.cpp:50-59 and :104-112 (tau3 = {-1,+1}, new_types/dirac.hpp:38-41;
+ * P+- = (1 +- i g5)/sqrt2, new_types/dirac.cpp:60-61), on an lx spinor */
+tms_status tms_rotate_twisted(tms_ctx *ctx, int r, const double *in_lx, double *out_lx);
+/* get_qprop (projects/ib/prop.cpp:41-112) without the photon and free-theory branches: the
+ * source rotated by P(r) when rotate_source (the reference's twisted_run), the solve
+ * (inv_tmclovD_cg_eoprec when cSW != 0, else inv_tmD_cg_eoprec), the sink rotated by P(r),
+ * all on the device */
+tms_status tms_get_qprop(tms_ctx *ctx, int r, int rotate_source, double kappa, int has_anis, double anis, double cSW,
+                         double mu, int niter, double residue, int precision, const double *src_lx, double *out_lx,
+                         tms_stats *stats);
+/* reconstruct_tm_doublet (dirac_operators/tmQ/reconstruct_tm_doublet.cpp:13-26; a stub there, whose
+ * commented body is followed): outminus = Q(+mu) in, outplus = outminus - 2 i mu in */
+tms_status tms_reconstruct_tm_doublet(tms_ctx *ctx, double kappa, int has_anis, double anis, double mu,
+                                      const double *in_lx, double *outminus_lx, double *outplus_lx);
+
 /* ---- gauge configuration files and checks ---- */
 
 /* read_ildg_gauge_conf (io/reader.hpp:75-99, io/ILDG_File.cpp): read the 'ildg-binary-data'

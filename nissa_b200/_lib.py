@@ -42,6 +42,9 @@ SIGNATURES = {
     "tms_apply_tmclovQ": (I, [P, D, I, D, D, P, P]),
     "tms_cg_tmclov_eoprec_square": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cg_tmclov_eoprec": (I, [P, P, P, D, I, D, D, D, I, D, I, ctypes.POINTER(Stats)]),
+    "tms_rotate_twisted": (I, [P, I, P, P]),
+    "tms_get_qprop": (I, [P, I, I, D, I, D, D, D, I, D, I, P, P, ctypes.POINTER(Stats)]),
+    "tms_reconstruct_tm_doublet": (I, [P, D, I, D, D, P, P, P]),
     "tms_read_ildg": (I, [P, ctypes.c_char_p, P]),
     "tms_write_ildg": (I, [P, ctypes.c_char_p, P, I]),
     "tms_conf_load_ildg": (I, [P, ctypes.c_char_p, I]),

@@ -156,6 +156,8 @@ tms_status tms_destroy(tms_ctx* ctx)
   fr(ctx->xlo32.n);
   fr(ctx->lx_of_eo);
   fr(ctx->U64);
+  fr(ctx->lxbuf[0]);
+  fr(ctx->lxbuf[1]);
   fr(ctx->cl64);
   fr(ctx->cl32);
   fr(ctx->icl64);

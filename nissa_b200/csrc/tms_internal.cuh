@@ -96,6 +96,9 @@ struct tms_ctx
   void* cgm_ps = nullptr;
   int cgm_prec = -1, cgm_nshift = 0;
 
+  // lx spinor buffers on the device for the propagator entry points (tms_prop.cu)
+  double* lxbuf[2] = {nullptr, nullptr};
+
   // twisted clover (tms_clover_term): the clover term of both parities and
   // the twisted inverse on even sites for (icl_kappa, icl_mu)
   bool clov_ok = false, icl_ok = false;

@@ -394,6 +394,40 @@ class Lattice:
     def batch_session(self, nslots: int, precision: str = "single", anis=None) -> BatchSession:
         return BatchSession(self, nslots, precision, anis)
 
+    # ------------------------------------------------- around a propagator solve
+    def rotate_twisted(self, r: int, inp, out=None):
+        """safe_dirac_prod_spincolor with P- (r=0) or P+ (r=1) on an lx spinor."""
+        return self._unary(self.lib.tms_rotate_twisted, lambda i, o: (int(r), i, o), inp, (self.V, 4, 3, 2), out)
+
+    def get_qprop(self, r: int, kappa, mu, source_lx, residue, cSW=0.0, rotate_source=True, niter=1000000,
+                  anis=None, precision="double", out=None, raise_on_error=True):
+        """get_qprop (projects/ib/prop.cpp:41-112): P(r) source -> solve -> P(r) sink.  Returns (prop, stats)."""
+        shape = (self.V, 4, 3, 2)
+        s = _Buf(source_lx, shape)
+        sol = self._new_out(source_lx, shape) if out is None else out
+        o = _Buf(sol, shape, out=True)
+        self._mode(s, o)
+        stats = _lib.Stats()
+        a = self._anis(anis)
+        st = self.lib.tms_get_qprop(self.h, int(r), 1 if rotate_source else 0, kappa, a[0], a[1], float(cSW), mu,
+                                    int(niter), float(residue), PRECISION[precision], s.ptr, o.ptr,
+                                    ctypes.byref(stats))
+        if raise_on_error:
+            self._check(st, "get_qprop", stats.as_dict(), sol)
+        return sol, stats.as_dict()
+
+    def reconstruct_tm_doublet(self, kappa, mu, inp, anis=None):
+        """(outminus, outplus) = (Q(+mu) in, Q(+mu) in - 2 i mu in)."""
+        shape = (self.V, 4, 3, 2)
+        i = _Buf(inp, shape)
+        om, op = self._new_out(inp, shape), self._new_out(inp, shape)
+        bm, bp = _Buf(om, shape, out=True), _Buf(op, shape, out=True)
+        self._mode(i, bm, bp)
+        a = self._anis(anis)
+        self._check(self.lib.tms_reconstruct_tm_doublet(self.h, kappa, a[0], a[1], mu, i.ptr, bm.ptr, bp.ptr),
+                    "reconstruct_tm_doublet")
+        return om, op
+
     # ------------------------------------------------------ twisted clover
     def clover_term(self, cSW: float):
         """clover_term(Cl, cSW, conf): computed and kept on the device for the resident conf."""
