@@ -581,6 +581,54 @@ def run_configs(args):
     print(json.dumps({"workload": "configurations below the headline volume", "results": res}), flush=True)
 
 
+CLOVER_WORKLOAD = dict(name="twisted-clover e/o CG solve (inv_tmclovD_cg_eoprec), 32^3x64, cSW 1.6, point sources, "
+                            "|r|/|b|<=1e-10", T=64, L=32, eps=0.35, seed=1, kappa=0.1350, cSW=1.6, mu=0.005,
+                       residue=1e-20)
+
+
+def run_clover(args):
+    """The twisted-clover full solve at the headline volume: FP64, FP32-inner and
+    FP16-inner (FP64 reliable updates), each solution's true residual checked
+    in FP64 and compared with the FP64 solve (an extra line, not the headline)."""
+    import torch
+    from nissa_b200 import Lattice
+    from nissa_b200 import workload as wl
+    W = dict(CLOVER_WORKLOAD)
+    if args.lattice:
+        W["T"], W["L"] = (int(x) for x in args.lattice.split(","))
+    T, L = W["T"], W["L"]
+    V = T * L ** 3
+    dev = "cuda:0"
+    lat = Lattice(T, L)
+    lat.upload_conf(wl.gauge_conf(T, L, W["eps"], W["seed"], device=dev))
+    t0 = time.perf_counter()
+    lat.clover_term(W["cSW"])
+    t_clover = time.perf_counter() - t0
+    src = torch.zeros((V, 4, 3, 2), dtype=torch.float64, device=dev)
+    src[0, 0, 0, 0] = 1.0
+    sols, res = {}, {}
+    for prec in ("double", "single", "half"):
+        sols[prec] = torch.empty_like(src)
+        lat.inv_tmclovD_cg_eoprec(W["kappa"], W["cSW"], W["mu"], src, 100000, W["residue"], precision=prec,
+                                  out=sols[prec])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, st = lat.inv_tmclovD_cg_eoprec(W["kappa"], W["cSW"], W["mu"], src, 100000, W["residue"], precision=prec,
+                                          out=sols[prec])
+        e1.record()
+        torch.cuda.synchronize()
+        res[prec] = {"ms_per_solve": e0.elapsed_time(e1), "iterations": st["iterations"],
+                     "reliable_updates": st["reliable_updates"], "true_rel_res2": st["true_rel_res2"],
+                     "lx_rel_res2": st["lx_rel_res2"]}
+    for prec in ("single", "half"):
+        res[prec]["rel_err_vs_fp64"] = float(torch.linalg.norm(sols[prec] - sols["double"]) /
+                                             torch.linalg.norm(sols["double"]))
+        res[prec]["speedup_vs_fp64"] = res["double"]["ms_per_solve"] / res[prec]["ms_per_solve"]
+    print(json.dumps({"workload": W["name"].replace("32^3x64", "%d^3x%d" % (L, T)), "kappa": W["kappa"],
+                      "cSW": W["cSW"], "mu": W["mu"], "clover_term_s": t_clover, "results": res}), flush=True)
+
+
 SERVE_WORKLOAD = dict(volumes={"8^3x16": (16, 8), "16^3x32": (32, 16), "32^3x64": (64, 32)},
                       probs=[0.5, 0.35, 0.15], eps=0.35, seed=1, rate=20.0, requests=200, nslots=16)
 
@@ -629,10 +677,11 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
     ap.add_argument("--hop-cfg", type=int, default=-1, help="hopping-kernel launch shape for --kernel-only (tuning)")
-    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve", "batched", "configs"],
+    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve", "batched", "configs", "clover"],
                     help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop; "
                          "batched: 48 right-hand sides batched vs one at a time; configs: the 8^3x16 and "
-                         "16^3x32 configurations with the reference's CPU solve (extra reports)")
+                         "16^3x32 configurations with the reference's CPU solve; clover: the twisted-clover "
+                         "solve (extra reports)")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--requests", type=int, default=0, help="serve: number of requests")
     ap.add_argument("--serve-precision", default="single", choices=["double", "single", "half"])
@@ -658,6 +707,9 @@ def main():
         return
     if args.workload == "configs":
         run_configs(args)
+        return
+    if args.workload == "clover":
+        run_clover(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)
