@@ -219,7 +219,7 @@ namespace tms
     const int n = FWD ? nbr_up<MU>(g, s, w) : nbr_dw<MU>(g, s, w);
     C<Re> L[9];
     Re ls;
-    U.load_scaled(FWD ? p : 1 - p, MU, FWD ? ieo : n, L, ls);
+    U.template load_scaled<false>(FWD ? p : 1 - p, MU, FWD ? ieo : n, L, ls);
     const Re f = (w ? fmu * Re(g.bc_t) : fmu) * ls;
 #pragma unroll
     for (int j = 0; j < R; j++)

@@ -249,7 +249,20 @@ namespace tms
   };
 
   // -------------------------------------------------------- link accessors
+  // Low-precision links are loaded with the streaming hint (evict first): each
+  // link is read once per hop, so it should not displace the neighbour
+  // spinors, which are read up to eight times, from L1 and L2.
   template <int F> struct LinkT;
+
+  // a link load: streaming (evict first) by default; kept cached when the
+  // same thread reuses the link (the batched kernel applies it to several
+  // right-hand sides one group after the other)
+  template <bool STREAM, class T>
+  __device__ __forceinline__ T ld_link(const T* p)
+  {
+    if (STREAM) return __ldcs(p);
+    return __ldg(p);
+  }
 
   template <> struct LinkT<LINK_F64_18>
   {
@@ -257,18 +270,20 @@ namespace tms
     const double2* __restrict__ d; // [par][mu][9][Vh]
     int Vh;
     // the link and a factor to apply to its products (1 here)
+    template <bool STREAM = true>
     __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<double> u[9], double& scale) const
     {
-      load(par, mu, site, u);
+      load<STREAM>(par, mu, site, u);
       scale = double(1);
     }
+    template <bool STREAM = true>
     __device__ __forceinline__ void load(int par, int mu, int site, C<double> u[9]) const
     {
       const double2* b = d + ((size_t)(par * 4 + mu) * 9) * Vh + site;
 #pragma unroll
       for (int k = 0; k < 9; k++)
         {
-          const double2 w = __ldg(b + (size_t)k * Vh);
+          const double2 w = ld_link<STREAM>(b + (size_t)k * Vh);
           u[k] = {w.x, w.y};
         }
     }
@@ -280,22 +295,25 @@ namespace tms
     const float2* __restrict__ d; // [par][mu][9][Vh]
     int Vh;
     // the link and a factor to apply to its products (1 here)
+    template <bool STREAM = true>
     __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<float> u[9], float& scale) const
     {
-      load(par, mu, site, u);
+      load<STREAM>(par, mu, site, u);
       scale = float(1);
     }
     // stored rows (all three) in stored units, for the two-site kernels
     static constexpr int kRows = 3;
     static constexpr float kUnit = 1.0f;
-    __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[9]) const { load(par, mu, site, u); }
+    template <bool STREAM = true>
+    __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[9]) const { load<STREAM>(par, mu, site, u); }
+    template <bool STREAM = true>
     __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
     {
       const float2* b = d + ((size_t)(par * 4 + mu) * 9) * Vh + site;
 #pragma unroll
       for (int k = 0; k < 9; k++)
         {
-          const float2 w = __ldg(b + (size_t)k * Vh);
+          const float2 w = ld_link<STREAM>(b + (size_t)k * Vh);
           u[k] = {w.x, w.y};
         }
     }
@@ -307,18 +325,20 @@ namespace tms
     const float4* __restrict__ d; // [par][mu][3][Vh]
     int Vh;
     // the link and a factor to apply to its products (1 here)
+    template <bool STREAM = true>
     __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<float> u[9], float& scale) const
     {
-      load(par, mu, site, u);
+      load<STREAM>(par, mu, site, u);
       scale = float(1);
     }
     // stored rows 0 and 1 in stored units, for the two-site kernels
     static constexpr int kRows = 2;
     static constexpr float kUnit = 1.0f;
+    template <bool STREAM = true>
     __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[6]) const
     {
       const float4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const float4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      const float4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
       u[0] = {a0.x, a0.y};
       u[1] = {a0.z, a0.w};
       u[2] = {a1.x, a1.y};
@@ -326,10 +346,11 @@ namespace tms
       u[4] = {a2.x, a2.y};
       u[5] = {a2.z, a2.w};
     }
+    template <bool STREAM = true>
     __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
     {
       const float4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const float4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      const float4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
       u[0] = {a0.x, a0.y};
       u[1] = {a0.z, a0.w};
       u[2] = {a1.x, a1.y};
@@ -351,10 +372,11 @@ namespace tms
     // stored rows 0 and 1 in raw 16-bit units (value = raw * kUnit), for the two-site kernels
     static constexpr int kRows = 2;
     static constexpr float kUnit = 1.0f / 32767.0f;
+    template <bool STREAM = true>
     __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[6]) const
     {
       const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const short4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      const short4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
       u[0] = {float(a0.x), float(a0.y)};
       u[1] = {float(a0.z), float(a0.w)};
       u[2] = {float(a1.x), float(a1.y)};
@@ -364,11 +386,12 @@ namespace tms
     }
     // rows 0 and 1 in raw 16-bit units, row 2 rebuilt from them and brought to
     // the same units: the products of this link are to be multiplied by `scale`
+    template <bool STREAM = true>
     __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<float> u[9], float& scale) const
     {
       constexpr float k = 1.0f / 32767.0f;
       const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const short4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      const short4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
       u[0] = {float(a0.x), float(a0.y)};
       u[1] = {float(a0.z), float(a0.w)};
       u[2] = {float(a1.x), float(a1.y)};
@@ -380,11 +403,12 @@ namespace tms
       u[8] = cscale(cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3]))), k);
       scale = k;
     }
+    template <bool STREAM = true>
     __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
     {
       constexpr float k = 1.0f / 32767.0f;
       const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const short4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+      const short4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
       u[0] = {a0.x * k, a0.y * k};
       u[1] = {a0.z * k, a0.w * k};
       u[2] = {a1.x * k, a1.y * k};
