@@ -68,8 +68,9 @@ namespace tms
     if (!last) return;
     __threadfence();
     double s = 0.0;
-    const volatile double* row = red.partial + (size_t)rhs * gridDim.x;
-    for (int i = lane; i < (int)gridDim.x; i += 32) s += row[i];
+    const double* row = red.partial + (size_t)rhs * gridDim.x;
+#pragma unroll 8
+    for (int i = lane; i < (int)gridDim.x; i += 32) s += __ldcg(row + i); // past L1, several in flight
     s = warp_sum(s);
     if (lane == 0)
       {

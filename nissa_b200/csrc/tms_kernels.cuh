@@ -56,8 +56,11 @@ namespace tms
     if (amLast)
       {
         __threadfence();
+        // the partials of the other blocks are in L2 (__threadfence before each
+        // ticket): load them past L1, several in flight, in a fixed order per thread
         double s = 0.0;
-        for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) s += ((volatile double*)red.partial)[i];
+#pragma unroll 8
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) s += __ldcg(red.partial + i);
         s = warp_sum(s);
         if (lane == 0) sh[warp] = s;
         __syncthreads();
