@@ -143,9 +143,11 @@ tms_status tms_cg_tmQ2(tms_ctx *ctx, double *sol_lx, const double *guess_lx, con
  * cgm_invert in inverters/templates/cgm_invert_template_threaded.hpp:11-295).
  * Solves (Q_W^2 + m_k^2) sol_k = src for nmass (<= 32) masses at once; sols is an array of nmass lx
  * spinors (nissa's spincolor**), residues the per-shift squared relative residues.  TMS_PREC_DOUBLE is
- * the reference's FP64 multi-shift CG; the mixed precisions run it in FP32 down to |r|/|b| = 1e-6 and
- * bring each shift to its target with the mixed-precision CG of tms_cg_tmQ2 from that guess, checking
- * every shift's true residual in FP64.  stats (may be NULL) receives nmass entries. */
+ * the reference's FP64 multi-shift CG; the mixed precisions run it in FP32 down to the squared residue
+ * "cgm_floor_single" (tms_set_tuning, default 1e-12) and bring each shift to its target by defect
+ * correction through the mixed-precision e/o solver (e = D(-m)^-1 g5 D(+m)^-1 g5 r, since
+ * Q_W^2 + m^2 = Q(+m) Q(-m) and Q = g5 D), checking every shift's true residual in FP64.
+ * stats (may be NULL) receives nmass entries. */
 tms_status tms_cgm_tmQ2(tms_ctx *ctx, double *const *sols, const double *src_lx, double kappa, int has_anis,
                         double anis, const double *masses, int nmass, int niter, const double *residues,
                         int precision, tms_stats *stats);

@@ -419,6 +419,12 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       ctx->graph_iters = v;
       return TMS_OK;
     }
+  if (k == "cgm_floor_single")
+    {
+      if (!(value >= 1e-20 && value < 1.0)) return fail(ctx, TMS_ERR_BAD_ARG, "cgm_floor_single: in [1e-20, 1)");
+      ctx->cgm_floor32 = value;
+      return TMS_OK;
+    }
   if (k == "batch_graph_iters")
     {
       const int v = (int)value;

@@ -569,6 +569,41 @@ tms_status tms_cg_eoprec_square(tms_ctx* ctx, double* sol, const double* guess, 
   return st;
 }
 
+} // extern "C"
+
+namespace
+{
+  // Eq. (8)-(11) of inv_tmD_cg_eoprec_native (cg_invert_tmD_eoprec.cpp:102-150) on
+  // device fields: the source's parities in ex[0] (even) and ex[1] (odd), the
+  // solution's in ex[2], ex[3].  The operator parameters must be set.
+  tms_status eo_full_solve(tms_ctx* ctx, int niter, double residue, int precision, tms_stats* stats)
+  {
+    Field* f = ctx->f64;
+    for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
+    Field *eta = ctx->ex, *psi = ctx->ex + 2; // [0] even, [1] odd
+    const int n = (int)ctx->g.Vh;
+    auto V = [&](const Field& x) { return view<PREC_F64>(x); };
+    auto U = links64(ctx);
+    // Eq. (8a): te = D_ee^-1 eta_e ; Eq. (8b): varphi = g5 (eta_o + hop(te)/2) -> f0
+    ++ctx->launches;
+    diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(eta[0]), V(f[5]), ctx->prm, 1.0, 1);
+    EpiSrcPrep<PREC_F64> sp{{V(f[0]), V(f[0])}, {V(eta[1]), V(eta[1])}};
+    launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
+    CU(cudaGetLastError());
+    // Eq. (9)
+    const tms_status st = cg_dispatch<EoOp>(ctx, precision, niter, residue, false, stats);
+    if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+    // Eq. (10): psi_o = K(-mu) x ; Eq. (11): psi_e = D_ee^-1 (eta_e + hop(psi_o)/2)
+    kern_op<PREC_F64>(ctx, U, f[1], f[5], psi[1], -1.0, ctx->prm);
+    EpiReco<PREC_F64> rc{{V(psi[0]), V(psi[0])}, {V(eta[0]), V(eta[0])}, ctx->prm, 1.0};
+    launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
+    CU(cudaGetLastError());
+    return st;
+  }
+}
+
+extern "C" {
+
 tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, double kappa, int has_anis, double anis,
                          double mu, int niter, double residue, int precision, tms_stats* stats)
 {
@@ -596,20 +631,8 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
   aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(eta[0]));
   ++ctx->launches;
   aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
-  // Eq. (8a): te = D_ee^-1 eta_e ; Eq. (8b): varphi = g5 (eta_o + hop(te)/2) -> f0
-  ++ctx->launches;
-  diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(eta[0]), V(f[5]), ctx->prm, 1.0, 1);
-  EpiSrcPrep<PREC_F64> sp{{V(f[0]), V(f[0])}, {V(eta[1]), V(eta[1])}};
-  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
-  CU(cudaGetLastError());
-  // Eq. (9)
-  const tms_status st = cg_dispatch<EoOp>(ctx, precision, niter, residue, false, stats);
+  const tms_status st = eo_full_solve(ctx, niter, residue, precision, stats);
   if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
-  // Eq. (10): psi_o = K(-mu) x ; Eq. (11): psi_e = D_ee^-1 (eta_e + hop(psi_o)/2)
-  kern_op<PREC_F64>(ctx, U, f[1], f[5], psi[1], -1.0, ctx->prm);
-  EpiReco<PREC_F64> rc{{V(psi[0]), V(psi[0])}, {V(eta[0]), V(eta[0])}, ctx->prm, 1.0};
-  launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
-  CU(cudaGetLastError());
   // paste_eo_parts_into_lx_vector
   double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sol_lx;
   ++ctx->launches;
@@ -770,9 +793,10 @@ tms_status tms_cgm_tmQ2(tms_ctx* ctx, double* const* sols, const double* src_lx,
   TRY(norm2<PREC_F64>(ctx, f[0], &b2, stride));
   if (b2 == 0.0 || std::isnan(b2)) return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm: %g", b2);
   double sigma[CGM_MAX_SHIFTS], target[CGM_MAX_SHIFTS];
-  // the FP32 multi-shift solve stops at |r|/|b| = 1e-6 at most; each shift is
-  // then brought to its target by the mixed-precision CG from that guess
-  const double floor32 = 1e-12;
+  // the FP32 multi-shift solve stops at the squared relative residue
+  // cgm_floor_single at most; each shift is then brought to its target by the
+  // mixed-precision CG from that guess
+  const double floor32 = ctx->cgm_floor32;
   for (int k = 0; k < nmass; k++)
     {
       sigma[k] = masses[k] * masses[k];
@@ -800,15 +824,56 @@ tms_status tms_cgm_tmQ2(tms_ctx* ctx, double* const* sols, const double* src_lx,
       fill_stats(&sk, st, iters, 0, ctx->cgm_h->res[k], rt / b2, ms);
       if (precision != TMS_PREC_DOUBLE && rt >= residues[k] * b2)
         {
-          tms_stats rs{};
-          const tms_status s2 = cg_dispatch<LxOp>(ctx, precision, niter, residues[k], true, &rs);
-          if (s2 != TMS_OK && s2 != TMS_ERR_NOT_CONVERGED) return s2;
+          // defect correction through the e/o solver, FP64 residuals in between:
+          // (Q_W^2 + m^2)^-1 = Q(-m)^-1 Q(+m)^-1 and Q(mu)^-1 = D(mu)^-1 g5, so
+          // e = D(-m)^-1 g5 D(+m)^-1 g5 r ; x += e ; r = b - (Q_W^2 + m^2) x
+          Field* ex = ctx->ex;
+          for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
+          const int n = (int)ctx->g.Vh;
+          tms_status s2 = TMS_OK;
+          int corrections = 0;
+          while (rt >= residues[k] * b2 && corrections < 4)
+            {
+              // each e/o solve to a hundredth of the remaining factor (squared residues)
+              const double rel = std::min(1e-2, std::max(1e-22, 1e-2 * residues[k] * b2 / rt));
+              for (int p = 0; p < 2; p++)
+                {
+                  ++ctx->launches;
+                  g5_copy_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+                    n, view_par<PREC_F64>(f[2], p), view<PREC_F64>(ex[p]));
+                }
+              for (int pass = 0; pass < 2; pass++)
+                {
+                  const double sg = pass ? -1.0 : +1.0;
+                  TRY(set_params(ctx, kappa, sg * masses[k], has_anis, anis));
+                  tms_stats es{};
+                  s2 = eo_full_solve(ctx, niter, rel, precision, &es);
+                  if (s2 != TMS_OK && s2 != TMS_ERR_NOT_CONVERGED) return s2;
+                  sk.iterations += es.iterations;
+                  sk.seconds += es.seconds;
+                  for (int p = 0; p < 2; p++)
+                    {
+                      ++ctx->launches;
+                      if (sg > 0)
+                        g5_copy_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+                          n, view<PREC_F64>(ex[2 + p]), view<PREC_F64>(ex[p]));
+                      else
+                        axpby_kernel<PREC_F64, PREC_F64, PREC_F64><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0,
+                                                                     ctx->stream>>>(
+                          n, 1.0, view_par<PREC_F64>(f[1], p), 1.0, view<PREC_F64>(ex[2 + p]),
+                          view_par<PREC_F64>(f[1], p));
+                    }
+                }
+              CU(cudaGetLastError());
+              TRY(set_params(ctx, kappa, masses[k], has_anis, anis));
+              TRY(LxOp::true_residual(ctx, f[0], f[1], f[2], &rt));
+              corrections++;
+            }
+          if (s2 == TMS_OK && rt >= residues[k] * b2) s2 = TMS_ERR_NOT_CONVERGED;
           if (s2 != TMS_OK) worst = s2;
-          sk.iterations += rs.iterations;
-          sk.reliable_updates = rs.reliable_updates;
-          sk.iterated_rel_res2 = rs.iterated_rel_res2;
-          sk.true_rel_res2 = rs.true_rel_res2;
-          sk.seconds += rs.seconds;
+          sk.reliable_updates = corrections;
+          sk.true_rel_res2 = rt / b2;
+          sk.iterated_rel_res2 = rt / b2;
           sk.status = s2;
         }
       if (stats) stats[k] = sk;

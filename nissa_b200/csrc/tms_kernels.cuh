@@ -1086,6 +1086,19 @@ namespace tms
     grid_reduce<BLAS_THREADS>(acc, red, NoFin{});
   }
 
+  // out = g5 in, FP64 (g5 = diag(1,1,-1,-1), new_types/dirac.cpp:48)
+  static __global__ void __launch_bounds__(BLAS_THREADS)
+    g5_copy_kernel(int n, SpinorT<PREC_F64> in, SpinorT<PREC_F64> out)
+  {
+    const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
+    if (i >= n) return;
+    C<double> u[12];
+    in.load(i, u);
+#pragma unroll
+    for (int c = 6; c < 12; c++) u[c] = {-u[c].re, -u[c].im};
+    out.store(i, u);
+  }
+
   // --------------------------------------------------- layout conversion
   // host-order AoS doubles (site-major, 24 per site) <-> SoA device spinor.
   // site_map (optional) gives the AoS row of SoA site i (used for lx <-> eo).
