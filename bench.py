@@ -314,6 +314,13 @@ def run_ours(args):
                    "sample": "reference inv_tmDkern_eoprec_square_eos_cg, %d iterations (+1 final residual) on the "
                              "same 32^3x64 conf, %.3f s/iteration, scaled by the %d FP64 iterations of a full solve"
                              % (CPU_SAMPLE_ITERS, spi, it64)}
+            # the reference's FP64 e/o Dslash on the same conf (3 repetitions), same bytes model
+            import oracle
+            if oracle.ref_available():
+                x = np.random.default_rng(6).standard_normal((V // 2, 4, 3, 2))
+                _, rec, _ = oracle.run_ref("hop", T, L, {"conf": conf_bc, "in": x}, (V // 2, 4, 3, 2), par=1, reps=3,
+                                           threads=cores)
+                cpu["dslash_gbs"] = d64_bytes / rec["seconds_per_rep"] / 1e9
         except Exception as e:  # the CPU baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable", "sample": str(e)}
 
