@@ -425,6 +425,13 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       ctx->cgm_floor32 = value;
       return TMS_OK;
     }
+  if (k == "pdl")
+    {
+      if (value != 0.0 && value != 1.0) return fail(ctx, TMS_ERR_BAD_ARG, "pdl: 0 or 1");
+      if (ctx->pdl != (int)value) drop_all();
+      ctx->pdl = (int)value;
+      return TMS_OK;
+    }
   if (k == "batch_graph_iters")
     {
       const int v = (int)value;

@@ -65,7 +65,8 @@ namespace
           launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
           const int n = nsites(c);
           ++c->launches;
-          xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s>>>(n, view<P>(r), view<P>(p), c->st, stop);
+          launch_pdl(c, xpay_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
+                     (const CgState*)c->st, stop);
         }
     }
   };
@@ -127,7 +128,8 @@ namespace
           launch_hop_v<P, LF>(c, s, 0, 2, V(t, 0), V(t, 1), U, prm, b, FinBeta{c->st}, stop);
           const int n = nsites(c);
           ++c->launches;
-          xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s>>>(n, view<P>(r), view<P>(p), c->st, stop);
+          launch_pdl(c, xpay_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
+                     (const CgState*)c->st, stop);
         }
     }
   };
@@ -182,7 +184,8 @@ namespace
           launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
           const int n = nsites(c);
           ++c->launches;
-          xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s>>>(n, view<P>(r), view<P>(p), c->st, stop);
+          launch_pdl(c, xpay_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
+                     (const CgState*)c->st, stop);
         }
     }
   };

@@ -97,6 +97,18 @@ namespace tms
     return lx >> 1;
   }
 
+  // ---------------------------------------- programmatic dependent launch
+  // A kernel launched with programmatic stream serialisation may start while
+  // its predecessor in the stream drains: it waits here, before reading
+  // anything the predecessor wrote, for the predecessor's completion and
+  // memory flush (a no-op for an ordinary launch), and lets its own successor
+  // start launching once all of its blocks have begun.
+  __device__ __forceinline__ void pdl_enter()
+  {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  }
+
   // ------------------------------------------------------- complex algebra
   template <typename R>
   struct C

@@ -123,6 +123,7 @@ struct tms_ctx
   double delta_single = 1e-3, delta_half = 0.005;
   int single_links16 = 0; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
   int mrhs_r = 1; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
+  int pdl = 1;    // launch the CG iteration kernels with programmatic dependent launch
   double cgm_floor32 = 1e-12; // squared residue at which the FP32 multi-shift phase hands over to refinement
 
   // batched-solver workspace (owned by tms_batch.cu)
@@ -214,6 +215,25 @@ namespace tms_int
   }
 
   // ------------------------------------------------------------ hop launch
+  // a launch with programmatic stream serialisation (when enabled): the kernel
+  // may start while its predecessor drains; it waits in pdl_enter()
+  template <typename... KArgs, typename... Args>
+  inline void launch_pdl(tms_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, cudaStream_t s,
+                         Args... args)
+  {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = c->pdl ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+  }
+
   template <int P, int LF, class Epi, class Fin = NoFin>
   void launch_hop_v(tms_ctx* c, cudaStream_t s, int par_out, int npar, const SpinorT<P>& in_e,
                     const SpinorT<P>& in_o, const LinkT<LF>& U, const OpParams* prm, const Epi& epi,
@@ -226,32 +246,32 @@ namespace tms_int
         {
           const int n2 = nsite / 2;
           if (c->hop_cfg[P] == 4)
-            hop2_kernel<P, LF, Epi, Fin><<<div_up(n2, HOP2_THREADS), HOP2_THREADS, 0, s>>>(
-              c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+            launch_pdl(c, hop2_kernel<P, LF, Epi, Fin>, div_up(n2, HOP2_THREADS), HOP2_THREADS, 0, s, c->g, par_out,
+                       npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
           else
             {
               constexpr int smem = PipeFmt<P, LF>::SMEM;
               static const cudaError_t attr = cudaFuncSetAttribute(
                 hop_pipe_kernel<P, LF, Epi, Fin>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
               (void)attr;
-              hop_pipe_kernel<P, LF, Epi, Fin><<<div_up(n2, PIPE_THREADS), PIPE_THREADS, smem, s>>>(
-                c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+              launch_pdl(c, hop_pipe_kernel<P, LF, Epi, Fin>, div_up(n2, PIPE_THREADS), PIPE_THREADS, smem, s, c->g,
+                         par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
             }
           return;
         }
     switch (c->hop_cfg[P])
       {
       case 1:
-        hop_kernel<P, LF, Epi, Fin, 1><<<div_up(nsite, HopCfg<P, 1>::NT), HopCfg<P, 1>::NT, 0, s>>>(
-          c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+        launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 1>, div_up(nsite, HopCfg<P, 1>::NT), HopCfg<P, 1>::NT, 0, s, c->g,
+                   par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
         break;
       case 2:
-        hop_kernel<P, LF, Epi, Fin, 2><<<div_up(nsite, HopCfg<P, 2>::NT), HopCfg<P, 2>::NT, 0, s>>>(
-          c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+        launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 2>, div_up(nsite, HopCfg<P, 2>::NT), HopCfg<P, 2>::NT, 0, s, c->g,
+                   par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
         break;
       default:
-        hop_kernel<P, LF, Epi, Fin, 0><<<div_up(nsite, HopCfg<P, 0>::NT), HopCfg<P, 0>::NT, 0, s>>>(
-          c->g, par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+        launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 0>, div_up(nsite, HopCfg<P, 0>::NT), HopCfg<P, 0>::NT, 0, s, c->g,
+                   par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
       }
   }
 

@@ -730,6 +730,7 @@ namespace tms
   {
     using R = typename SpinorT<P>::R;
     constexpr int NT = HopCfg<P, CFG>::NT;
+    pdl_enter();
     if (stop && *stop) return;
     const int idx = blockIdx.x * NT + threadIdx.x;
     int p = par_out, ieo = idx;
@@ -926,6 +927,7 @@ namespace tms
     hop2_kernel(Lattice g, int par_out, int npar, SpinorT<P> in_e, SpinorT<P> in_o, LinkT<LF> U, const OpParams* prm,
                 Epi epi, Reducer red, Fin fin, const int* __restrict__ stop)
   {
+    pdl_enter();
     if (stop && *stop) return;
     const int hv = (int)(g.Vh >> 1);
     const int idx = blockIdx.x * HOP2_THREADS + threadIdx.x;
@@ -975,6 +977,7 @@ namespace tms
     xpay_kernel(int n, SpinorT<P> r, SpinorT<P> p, const CgState* st, const int* __restrict__ stop)
   {
     using R = typename SpinorT<P>::R;
+    pdl_enter();
     if (stop && *stop) return;
     const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
     if (i >= n) return;

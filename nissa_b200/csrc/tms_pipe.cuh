@@ -279,6 +279,7 @@ namespace tms
   {
     using F = PipeFmt<P, LF>;
     extern __shared__ __align__(16) unsigned char pipe_smem[];
+    pdl_enter();
     if (stop && *stop) return;
     const int hv = (int)(g.Vh >> 1);
     const int idx = blockIdx.x * PIPE_THREADS + threadIdx.x;
