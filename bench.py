@@ -195,6 +195,7 @@ def run_ours(args):
     lat = Lattice(T, L, bc_t=W["bc_t"], device=local)
     lat.upload_conf(conf)
     assert lat.conf_is_su3
+    plaquette = lat.plaquette()  # global_plaquette_lx_conf of the periodic links, on the device
 
     def column(k):
         s = torch.zeros((V, 4, 3, 2), dtype=torch.float64, device=dev)
@@ -335,7 +336,8 @@ def run_ours(args):
         "dtype": PREC_DTYPE[prec],
         "data": "synthetic (seeded gauge recipe U=exp(i eps H), point sources)",
         "config": {"workload": W["name"], "T": T, "L": L, "kappa": kappa, "mu": mu, "eps": W["eps"],
-                   "residue_sq": residue, "sources": "12 point spin-colour columns at the origin, cycled",
+                   "residue_sq": residue, "plaquette": plaquette,
+                   "sources": "12 point spin-colour columns at the origin, cycled",
                    "inner_precision": prec,
                    "l2": "working set (links 0.2-0.4 GB + spinors) larger than the 126 MB L2",
                    "parallelism": "replicas" if ws > 1 else "1 GPU"},
