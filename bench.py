@@ -48,7 +48,7 @@ METRIC = "CG solves/s & Dslash HBM GB/s, 32³×64 mixed vs FP64 @1e-10; p50/p99 
 UNIT = "solves/s"
 CPU_SAMPLE_ITERS = 20
 HOP_KERNEL = {"half": "hop_kernel<FP16 spinors, 16-bit 12-real links> + inverse diagonal (first half of K)",
-              "single": "hop_kernel<FP32 spinors, FP32 12-real links> + inverse diagonal (first half of K)"}
+              "single": "hop_kernel<FP32 spinors, 16-bit 12-real links> + inverse diagonal (first half of K)"}
 # DRAM bytes of one launch of that kernel on this workload, from ncu
 HOP_TRAFFIC = {"half": 298.2e6}
 
@@ -293,8 +293,8 @@ def run_ours(args):
 
     # --- the other inner precisions on the same solves (solver-reported device seconds) -----
     variants = {}
-    for name, vp, links16 in (("single", "single", 0), ("single_links16", "single", 1), ("half", "half", 0)):
-        if vp == prec and not links16:
+    for name, vp, links16 in (("single_links32", "single", 0), ("single", "single", 1), ("half", "half", 1)):
+        if vp == prec and (links16 or vp == "half"):
             continue
         lat.set_tuning("links_single", links16)
         solve(0, precision=vp)
@@ -302,7 +302,7 @@ def run_ours(args):
         variants[name] = {"solves_per_s": 1.0 / statistics.mean(x["seconds"] for x in vs),
                           "iterations": vs[0]["iterations"], "reliable_updates": vs[0]["reliable_updates"],
                           "true_rel_res2_max": max(x["true_rel_res2"] for x in vs)}
-    lat.set_tuning("links_single", 0)
+    lat.set_tuning("links_single", 1)
 
     # --- CPU baseline: the reference's own CG on a bounded sample (rank 0, N=1 only) ---------
     cpu = None

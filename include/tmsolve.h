@@ -43,7 +43,7 @@ typedef enum
 typedef enum
 {
   TMS_PREC_DOUBLE = 0,      /* plain FP64 CG, the reference's arithmetic */
-  TMS_PREC_MIXED_SINGLE = 1,/* FP32 inner CG, 12-real links, FP64 reliable updates */
+  TMS_PREC_MIXED_SINGLE = 1,/* FP32 inner CG, 12-real 16-bit (or FP32) links, FP64 reliable updates */
   TMS_PREC_MIXED_HALF = 2   /* FP16 spinors with per-site FP32 scale, FP64 reliable updates */
 } tms_precision;
 
@@ -267,7 +267,7 @@ uint64_t tms_launch_count(const tms_ctx *ctx);
  * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
  * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
  * dropped by this factor, 0 < delta < 1), "links_single" (0: the FP32-spinor inner solver reads FP32
- * 12-real links, 1: 16-bit fixed-point 12-real links), "mrhs_per_thread" (right-hand sides one thread of the
+ * 12-real links, 1 (default): 16-bit fixed-point 12-real links), "mrhs_per_thread" (right-hand sides one thread of the
  * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2),
  * "batch_graph_iters" (CG iterations per batch-session graph block, 0: chosen by batch size).  Results do not depend on the launch shapes. */
 tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);

@@ -121,7 +121,7 @@ struct tms_ctx
   // reliable-update trigger of the mixed solvers
   int hop_cfg[3] = {0, 1, 0};
   double delta_single = 1e-3, delta_half = 0.005;
-  int single_links16 = 0; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
+  int single_links16 = 1; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
   int mrhs_r = 1; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
   int pdl = 1;    // launch the CG iteration kernels with programmatic dependent launch
   double cgm_floor32 = 1e-12; // squared residue at which the FP32 multi-shift phase hands over to refinement
