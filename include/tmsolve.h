@@ -131,6 +131,17 @@ tms_status tms_cg_eoprec_square(tms_ctx *ctx, double *sol, const double *guess, 
  * Full solve D_tm sol = src on lx spinors via Eq. (8)-(11) of the e/o preconditioning. */
 tms_status tms_cg_eoprec(tms_ctx *ctx, double *sol_lx, const double *src_lx, double kappa, int has_anis,
                          double anis, double mu, int niter, double residue, int precision, tms_stats *stats);
+/* inv_tmD_cg_eoprec for ncols sources one after the other (the loop over the 12 spin-colour columns
+ * of a propagator, projects/ib/prop.cpp:41-112, calls it once per column).  Each column is the same
+ * solve as tms_cg_eoprec; with host pointers the copy of column k+1's source in and of column k-1's
+ * solution out run on a copy stream while column k is solved (page-locked host buffers overlap,
+ * pageable ones are copied all the same).  sols_lx/srcs_lx are arrays of ncols lx spinors; stats
+ * (may be NULL) receives ncols entries.  Returns the first error, else TMS_ERR_NOT_CONVERGED if a
+ * column did not converge (its solution is still written), else TMS_OK; no copy into or out of the
+ * caller's buffers is left running when it returns. */
+tms_status tms_cg_eoprec_columns(tms_ctx *ctx, int ncols, double *const *sols_lx, const double *const *srcs_lx,
+                                 double kappa, int has_anis, double anis, double mu, int niter, double residue,
+                                 int precision, tms_stats *stats);
 
 /* inv_tmQ2_cg: inverters/twisted_mass/cg_invert_tmQ2_common.cpp:5 (a CRASH("reimplement") stub in the
  * reference, cg_invert_tmQ2.cpp:12-14).  Full-lattice CG on Q(+m)Q(-m) = Q_W^2 + m^2 (lx spinors);
@@ -267,7 +278,9 @@ uint64_t tms_launch_count(const tms_ctx *ctx);
  * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
  * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
  * dropped by this factor, 0 < delta < 1), "links_single" (0: the FP32-spinor inner solver reads FP32
- * 12-real links, 1 (default): 16-bit fixed-point 12-real links), "mrhs_per_thread" (right-hand sides one thread of the
+ * 12-real links, 1 (default): 16-bit fixed-point 12-real links), "links_reliable" (1 (default): the FP64
+ * residual recomputations of the mixed solvers read the links as 12 reals, row 2 rebuilt, when the conf
+ * is SU(3) to 1e-13; 0: always 18 reals), "mrhs_per_thread" (right-hand sides one thread of the
  * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2),
  * "batch_graph_iters" (CG iterations per batch-session graph block, 0: chosen by batch size).  Results do not depend on the launch shapes. */
 tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);

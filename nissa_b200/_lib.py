@@ -61,6 +61,7 @@ SIGNATURES = {
     "tms_cg_tmQ2": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cgm_tmQ2": (I, [P, P, P, D, I, D, P, I, I, P, I, P]),
     "tms_cg_eoprec_batched": (I, [P, I, P, P, D, I, D, P, I, P, I, P]),
+    "tms_cg_eoprec_columns": (I, [P, I, P, P, D, I, D, D, I, D, I, P]),
     "tms_batch_open": (I, [P, I, I, I, D, ctypes.POINTER(P)]),
     "tms_batch_submit": (I, [P, I, P, D, D, I, D]),
     "tms_batch_step": (I, [P, P, ctypes.POINTER(I)]),

@@ -108,11 +108,16 @@ tms_status tms_create4(tms_ctx** out, int T, int LX, int LY, int LZ, double bc_t
       cudaMalloc(&ctx->red_partial, sizeof(double) * ctx->red_cap) != cudaSuccess ||
       cudaMalloc(&ctx->red_counter, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&ctx->red_result, sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&ctx->st_h, sizeof(CgState)) != cudaSuccess ||
+      cudaHostAlloc(&ctx->st_h, sizeof(CgState), cudaHostAllocMapped) != cudaSuccess ||
       cudaMalloc(&ctx->cgm, sizeof(CgmState)) != cudaSuccess ||
       cudaMallocHost(&ctx->cgm_h, sizeof(CgmState)) != cudaSuccess ||
-      cudaMallocHost(&ctx->red_h, sizeof(double)) != cudaSuccess)
+      cudaHostAlloc(&ctx->red_h, sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostAlloc(&ctx->hring, kHostRing, cudaHostAllocMapped) != cudaSuccess)
     return cleanup(TMS_ERR_OOM);
+  if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->st_hd), ctx->st_h, 0) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->red_hd), ctx->red_h, 0) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->hring_d), ctx->hring, 0) != cudaSuccess)
+    return cleanup(TMS_ERR_CUDA);
   cudaMemset(ctx->red_counter, 0, sizeof(unsigned));
   cudaMemset(ctx->st, 0, sizeof(CgState));
   cudaEventCreate(&ctx->ev0);
@@ -135,6 +140,7 @@ tms_status tms_destroy(tms_ctx* ctx)
   if (!ctx) return TMS_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->cstream) cudaStreamSynchronize(ctx->cstream);
   for (auto& gr : ctx->graph)
     if (gr) cudaGraphExecDestroy(gr);
   auto fr = [](void* p) {
@@ -171,8 +177,13 @@ tms_status tms_destroy(tms_ctx* ctx)
   fr(ctx->red_counter);
   fr(ctx->red_result);
   fr(ctx->stage);
+  for (double*& b : ctx->colbuf) fr(b);
+  for (cudaEvent_t& e : ctx->colev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
   if (ctx->st_h) cudaFreeHost(ctx->st_h);
   if (ctx->red_h) cudaFreeHost(ctx->red_h);
+  if (ctx->hring) cudaFreeHost(ctx->hring);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -241,6 +252,7 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
   const double dev = read_result(ctx);
   CU(cudaGetLastError());
   ctx->su3 = (dev < 1e-10);
+  ctx->su3_dev = dev;
   ctx->conf_loaded = true;
   ctx->clov_ok = ctx->icl_ok = false; // a clover term belongs to the conf it was computed from
   return TMS_OK;
@@ -457,6 +469,12 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       if (value != 0.0 && value != 1.0) return fail(ctx, TMS_ERR_BAD_ARG, "links_single: 0 (FP32) or 1 (16-bit)");
       if (ctx->single_links16 != (int)value) drop_all();
       ctx->single_links16 = (int)value;
+      return TMS_OK;
+    }
+  if (k == "links_reliable")
+    {
+      if (value != 0.0 && value != 1.0) return fail(ctx, TMS_ERR_BAD_ARG, "links_reliable: 0 (18 reals) or 1 (12)");
+      ctx->reliable_links12 = (int)value;
       return TMS_OK;
     }
   if (k == "reliable_delta_single" || k == "reliable_delta_half")

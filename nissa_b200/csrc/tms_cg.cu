@@ -30,13 +30,24 @@ namespace
     static int& lo_prec(tms_ctx* c) { return c->lo_prec; }
     static Field& xlo(tms_ctx* c) { return c->xlo32; }
 
-    // r = b - K(+mu)K(-mu) x in FP64; returns |r|^2 (uses hi 4, 5, 6)
-    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr)
+    // r = b - K(+mu)K(-mu) x in FP64; returns |r|^2 (uses hi 4, 5, 6).  For the
+    // mixed solvers (`mixed`) the links may be read as 12 reals.
+    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr,
+                                    bool mixed = false)
     {
       Field &t1 = ctx->f64[4], &te = ctx->f64[5], &s = ctx->f64[6];
-      auto U = links64(ctx);
-      kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
-      kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
+      if (mixed && reliable_links12(ctx))
+        {
+          auto U = links64r(ctx);
+          kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
+          kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
+        }
+      else
+        {
+          auto U = links64(ctx);
+          kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
+          kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
+        }
       const int n = nsites(ctx);
       ++ctx->launches;
       residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
@@ -90,8 +101,9 @@ namespace
       launch_hop_v<P, LINK_F64_18>(c, s, 0, 2, view_par<P>(in, 0), view_par<P>(in, 1), links64(c), prm, e);
     }
 
-    // r = b - Q(+mu)Q(-mu) x in FP64; returns |r|^2 (uses hi 4, 5)
-    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr)
+    // r = b - Q(+mu)Q(-mu) x in FP64; returns |r|^2 (uses hi 4, 5); 18-real links always
+    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr,
+                                    bool = false)
     {
       Field &t = ctx->lx64[4], &s = ctx->lx64[5];
       qop<PREC_F64>(ctx, ctx->stream, x, t, -1.0, ctx->prm);
@@ -147,13 +159,24 @@ namespace
     static int& lo_prec(tms_ctx* c) { return c->lo_prec; }
     static Field& xlo(tms_ctx* c) { return c->xlo32; }
 
-    // r = b - K(false)K(true) x in FP64; returns |r|^2 (uses hi 4, 5, 6)
-    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr)
+    // r = b - K(false)K(true) x in FP64; returns |r|^2 (uses hi 4, 5, 6).  For the
+    // mixed solvers (`mixed`) the links may be read as 12 reals.
+    static tms_status true_residual(tms_ctx* ctx, const Field& b, const Field& x, const Field& r, double* rr,
+                                    bool mixed = false)
     {
       Field &t1 = ctx->f64[4], &te = ctx->f64[5], &s = ctx->f64[6];
-      auto U = links64(ctx);
-      clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), x, te, t1, 1, ctx->prm);
-      clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), t1, te, s, 0, ctx->prm);
+      if (mixed && reliable_links12(ctx))
+        {
+          auto U = links64r(ctx);
+          clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), x, te, t1, 1, ctx->prm);
+          clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), t1, te, s, 0, ctx->prm);
+        }
+      else
+        {
+          auto U = links64(ctx);
+          clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), x, te, t1, 1, ctx->prm);
+          clov_kern_op<PREC_F64>(ctx, U, clov64(ctx), t1, te, s, 0, ctx->prm);
+        }
       const int n = nsites(ctx);
       ++ctx->launches;
       residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
@@ -331,7 +354,7 @@ namespace
     TRY(norm2<PREC_F64>(ctx, f[0], &b2, n));
     if (b2 == 0.0 || std::isnan(b2)) return fail(ctx, TMS_ERR_INVALID_SOURCE, "invalid norm: %g", b2);
     double rr;
-    if (have_guess) TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rr));
+    if (have_guess) TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rr, true));
     else
       {
         CU(cudaMemsetAsync(f[1].d, 0, f[1].bytes, ctx->stream));
@@ -379,7 +402,7 @@ namespace
             CU(cudaMemsetAsync(xlo.d, 0, xlo.bytes, ctx->stream));
             if (xlo.n) CU(cudaMemsetAsync(xlo.n, 0, sizeof(float) * xlo.stride, ctx->stream));
             double rt;
-            TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rt));
+            TRY(Op::true_residual(ctx, f[0], f[1], f[2], &rt, true));
             reliable++;
             last_rt = rt; // the true residual of the current x
             if (rt < target) break;
@@ -407,7 +430,7 @@ namespace
       }
     // the last reliable update left x with its FP64 true residual; otherwise recompute it
     double tr = last_rt;
-    if (tr < 0.0) TRY(Op::true_residual(ctx, f[0], f[1], f[6], &tr));
+    if (tr < 0.0) TRY(Op::true_residual(ctx, f[0], f[1], f[6], &tr, true));
     fill_stats(stats, st, S.iter, reliable, S.rr / b2, tr / b2, ms);
     return st;
   }
@@ -605,6 +628,119 @@ namespace
   }
 }
 
+namespace
+{
+  // inv_tmD_cg_eoprec between AoS lx spinors in device memory (the operator
+  // parameters set): split the source into its parities, Eq. (8)-(11), paste
+  // the solution's parities, then the reference's lx residual check.  When
+  // given, `src_read` is recorded on the stream once the source has been read
+  // and `dst_ready` once the solution is written.
+  tms_status cg_eoprec_lx(tms_ctx* ctx, double* dst, const double* src, int niter, double residue, int precision,
+                          tms_stats* stats, cudaEvent_t src_read, cudaEvent_t dst_ready)
+  {
+    Field* f = ctx->f64;
+    for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
+    Field *eta = ctx->ex, *psi = ctx->ex + 2; // [0] even, [1] odd
+    for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
+    const int64_t Vh = ctx->g.Vh;
+    const int n = (int)Vh;
+    auto V = [&](const Field& x) { return view<PREC_F64>(x); };
+    // split_lx_vector_into_eo_parts(source)
+    ++ctx->launches;
+    aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(eta[0]));
+    ++ctx->launches;
+    aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
+    CU(cudaGetLastError());
+    if (src_read) CU(cudaEventRecord(src_read, ctx->stream));
+    const tms_status st = eo_full_solve(ctx, niter, residue, precision, stats);
+    if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+    // paste_eo_parts_into_lx_vector
+    ++ctx->launches;
+    soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, dst);
+    ++ctx->launches;
+    soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, dst);
+    CU(cudaGetLastError());
+    if (dst_ready) CU(cudaEventRecord(dst_ready, ctx->stream));
+    // lx residual check (cg_invert_tmD_eoprec.cpp:192-212): |g5 Q sol - src|^2 / |src|^2
+    if (stats)
+      {
+        EpiTmQ<PREC_F64, false> e{{V(f[2]), V(f[3])}, {V(psi[0]), V(psi[1])}, ctx->prm, +1.0};
+        launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 2, psi[0], psi[1], links64(ctx), ctx->prm, e);
+        double num = 0, den = 0;
+        for (int par = 0; par < 2; par++)
+          {
+            ++ctx->launches;
+            g5_residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, V(f[2 + par]),
+                                                                                         V(eta[par]), reducer(ctx));
+            CU(cudaGetLastError());
+            num += read_result(ctx);
+            double e2;
+            TRY(norm2<PREC_F64>(ctx, eta[par], &e2));
+            den += e2;
+          }
+        stats->lx_rel_res2 = num / den;
+      }
+    return st;
+  }
+
+  // the copy stream, the staging buffers and the events of pipelined column solves
+  tms_status ensure_columns(tms_ctx* ctx, size_t bytes)
+  {
+    if (!ctx->cstream) CU(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : ctx->colev)
+      if (!e) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (ctx->colbuf_bytes >= bytes) return TMS_OK;
+    for (double*& b : ctx->colbuf)
+      {
+        if (b) cudaFree(b);
+        b = nullptr;
+      }
+    ctx->colbuf_bytes = 0;
+    for (double*& b : ctx->colbuf) CU(cudaMalloc(&b, bytes));
+    ctx->colbuf_bytes = bytes;
+    return TMS_OK;
+  }
+
+  // Column k's source is copied in while column k-1 is solved, and its solution
+  // copied out while column k+1 is solved: two staging buffers each way on a
+  // copy stream, ordered against the solver's stream by events.
+  tms_status columns_host(tms_ctx* ctx, int ncols, double* const* sols, const double* const* srcs, int niter,
+                          double residue, int precision, tms_stats* stats, size_t bytes)
+  {
+    cudaEvent_t* in_ready = ctx->colev;
+    cudaEvent_t* in_free = ctx->colev + 2;
+    cudaEvent_t* out_ready = ctx->colev + 4;
+    cudaEvent_t* out_free = ctx->colev + 6;
+    double** in = ctx->colbuf;
+    double** out = ctx->colbuf + 2;
+    cudaStream_t cs = ctx->cstream;
+    CU(cudaMemcpyAsync(in[0], srcs[0], bytes, cudaMemcpyHostToDevice, cs));
+    CU(cudaEventRecord(in_ready[0], cs));
+    tms_status worst = TMS_OK;
+    for (int k = 0; k < ncols; k++)
+      {
+        const int b = k & 1;
+        if (k + 1 < ncols)
+          {
+            const int nb = (k + 1) & 1;
+            if (k >= 1) CU(cudaStreamWaitEvent(cs, in_free[nb], 0)); // column k-1 has read it
+            CU(cudaMemcpyAsync(in[nb], srcs[k + 1], bytes, cudaMemcpyHostToDevice, cs));
+            CU(cudaEventRecord(in_ready[nb], cs));
+          }
+        CU(cudaStreamWaitEvent(ctx->stream, in_ready[b], 0));
+        if (k >= 2) CU(cudaStreamWaitEvent(ctx->stream, out_free[b], 0)); // column k-2 has been copied out
+        const tms_status st = cg_eoprec_lx(ctx, out[b], in[b], niter, residue, precision, stats ? stats + k : nullptr,
+                                           in_free[b], out_ready[b]);
+        if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+        if (st != TMS_OK) worst = st;
+        CU(cudaStreamWaitEvent(cs, out_ready[b], 0));
+        CU(cudaMemcpyAsync(sols[k], out[b], bytes, cudaMemcpyDeviceToHost, cs));
+        CU(cudaEventRecord(out_free[b], cs));
+      }
+    return worst;
+  }
+}
+
 extern "C" {
 
 tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, double kappa, int has_anis, double anis,
@@ -613,56 +749,52 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
   TRY(check_conf(ctx));
   if (!sol_lx || !src_lx || niter <= 0 || !(residue > 0)) return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
   TRY(set_params(ctx, kappa, mu, has_anis, anis));
-  Field* f = ctx->f64;
-  for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
-  Field *eta = ctx->ex, *psi = ctx->ex + 2; // [0] even, [1] odd
-  for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
-  const int64_t Vh = ctx->g.Vh;
-  const int n = (int)Vh;
   const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
-  auto V = [&](const Field& x) { return view<PREC_F64>(x); };
-  auto U = links64(ctx);
-  // split_lx_vector_into_eo_parts(source)
   const double* src = src_lx;
+  double* dst = sol_lx;
   if (ctx->ptr_mode == TMS_PTR_HOST)
     {
       TRY(ensure_stage(ctx, bytes));
       CU(cudaMemcpyAsync(ctx->stage, src_lx, bytes, cudaMemcpyHostToDevice, ctx->stream));
-      src = ctx->stage;
+      src = dst = ctx->stage; // the source is split before the solution is pasted
     }
-  ++ctx->launches;
-  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(eta[0]));
-  ++ctx->launches;
-  aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
-  const tms_status st = eo_full_solve(ctx, niter, residue, precision, stats);
+  const tms_status st = cg_eoprec_lx(ctx, dst, src, niter, residue, precision, stats, nullptr, nullptr);
   if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
-  // paste_eo_parts_into_lx_vector
-  double* d = (ctx->ptr_mode == TMS_PTR_HOST) ? ctx->stage : sol_lx;
-  ++ctx->launches;
-  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, d);
-  ++ctx->launches;
-  soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, d);
-  CU(cudaGetLastError());
   if (ctx->ptr_mode == TMS_PTR_HOST) CU(cudaMemcpyAsync(sol_lx, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-  // lx residual check (cg_invert_tmD_eoprec.cpp:192-212): |g5 Q sol - src|^2 / |src|^2
-  if (stats)
+  TRY(finish(ctx));
+  return st;
+}
+
+tms_status tms_cg_eoprec_columns(tms_ctx* ctx, int ncols, double* const* sols_lx, const double* const* srcs_lx,
+                                 double kappa, int has_anis, double anis, double mu, int niter, double residue,
+                                 int precision, tms_stats* stats)
+{
+  TRY(check_conf(ctx));
+  if (ncols <= 0 || !sols_lx || !srcs_lx || niter <= 0 || !(residue > 0))
+    return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
+  for (int k = 0; k < ncols; k++)
+    if (!sols_lx[k] || !srcs_lx[k]) return fail(ctx, TMS_ERR_BAD_ARG, "column %d: null pointer", k);
+  TRY(set_params(ctx, kappa, mu, has_anis, anis));
+  tms_status st = TMS_OK;
+  if (ctx->ptr_mode == TMS_PTR_DEVICE)
     {
-      EpiTmQ<PREC_F64, false> e{{V(f[2]), V(f[3])}, {V(psi[0]), V(psi[1])}, ctx->prm, +1.0};
-      launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 2, psi[0], psi[1], U, ctx->prm, e);
-      double num = 0, den = 0;
-      for (int par = 0; par < 2; par++)
+      for (int k = 0; k < ncols; k++)
         {
-          ++ctx->launches;
-          g5_residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, V(f[2 + par]), V(eta[par]),
-                                                                                       reducer(ctx));
-          CU(cudaGetLastError());
-          num += read_result(ctx);
-          double e2;
-          TRY(norm2<PREC_F64>(ctx, eta[par], &e2));
-          den += e2;
+          const tms_status s = cg_eoprec_lx(ctx, sols_lx[k], srcs_lx[k], niter, residue, precision,
+                                            stats ? stats + k : nullptr, nullptr, nullptr);
+          if (s != TMS_OK && s != TMS_ERR_NOT_CONVERGED) return s;
+          if (s != TMS_OK) st = s;
         }
-      stats->lx_rel_res2 = num / den;
+      TRY(finish(ctx));
+      return st;
     }
+  const size_t bytes = (size_t)ctx->g.V * 24 * sizeof(double);
+  TRY(ensure_columns(ctx, bytes));
+  st = columns_host(ctx, ncols, sols_lx, srcs_lx, niter, residue, precision, stats, bytes);
+  // no copy into or out of the caller's buffers outlives the call, whatever the outcome
+  const cudaError_t e = cudaStreamSynchronize(ctx->cstream);
+  if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+  if (e != cudaSuccess) return fail(ctx, TMS_ERR_CUDA, "column copies: %s", cudaGetErrorString(e));
   TRY(finish(ctx));
   return st;
 }

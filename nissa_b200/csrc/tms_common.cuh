@@ -28,7 +28,7 @@
 namespace tms
 {
   enum Prec { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2 };
-  enum LinkFmt { LINK_F64_18 = 0, LINK_F32_12 = 1, LINK_F32_18 = 2, LINK_I16_12 = 3 };
+  enum LinkFmt { LINK_F64_18 = 0, LINK_F32_12 = 1, LINK_F32_18 = 2, LINK_I16_12 = 3, LINK_F64_12 = 4 };
 
   // ------------------------------------------------------------- geometry
   struct Lattice
@@ -298,6 +298,37 @@ namespace tms
           const double2 w = ld_link<STREAM>(b + (size_t)k * Vh);
           u[k] = {w.x, w.y};
         }
+    }
+  };
+
+  // The FP64 links read as 12 reals: rows 0 and 1 from the first six planes of
+  // the 18-real array, row 2 = conj(row0 x row1), which for links that are
+  // SU(3) to FP64 rounding is the stored row to rounding (a third less link
+  // traffic for the residual recomputations of the mixed solvers)
+  template <> struct LinkT<LINK_F64_12>
+  {
+    using R = double;
+    const double2* __restrict__ d; // [par][mu][9][Vh], planes 6-8 not read
+    int Vh;
+    template <bool STREAM = true>
+    __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<double> u[9], double& scale) const
+    {
+      load<STREAM>(par, mu, site, u);
+      scale = double(1);
+    }
+    template <bool STREAM = true>
+    __device__ __forceinline__ void load(int par, int mu, int site, C<double> u[9]) const
+    {
+      const double2* b = d + ((size_t)(par * 4 + mu) * 9) * Vh + site;
+#pragma unroll
+      for (int k = 0; k < 6; k++)
+        {
+          const double2 w = ld_link<STREAM>(b + (size_t)k * Vh);
+          u[k] = {w.x, w.y};
+        }
+      u[6] = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
+      u[7] = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));
+      u[8] = cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));
     }
   };
 

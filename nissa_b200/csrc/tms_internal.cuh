@@ -71,6 +71,16 @@ struct tms_ctx
   double* red_result = nullptr;
   double* red_h = nullptr;       // pinned
   int red_cap = 0;
+  // Scalars cross between host and device through mapped page-locked memory
+  // and a one-block copy kernel on the stream, not through the copy engines,
+  // which may be busy with the column copies of the copy stream: st_h and
+  // red_h are mapped (device addresses st_hd, red_hd); host->device scalars
+  // are staged in the ring hring (device address hring_d).
+  CgState* st_hd = nullptr;
+  double* red_hd = nullptr;
+  unsigned char* hring = nullptr;
+  unsigned char* hring_d = nullptr;
+  size_t hring_off = 0;
 
   // staging for AoS conversions (device AoS doubles), grows on demand
   double* stage = nullptr;
@@ -122,6 +132,8 @@ struct tms_ctx
   int hop_cfg[3] = {0, 1, 0};
   double delta_single = 1e-3, delta_half = 0.005;
   int single_links16 = 1; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
+  int reliable_links12 = 1; // FP64 residuals of the mixed solvers on 12-real FP64 links (when SU(3) to rounding)
+  double su3_dev = 1.0;     // largest deviation of the resident links from SU(3) (unitarity, row 2)
   int mrhs_r = 1; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
   int pdl = 1;    // launch the CG iteration kernels with programmatic dependent launch
   double cgm_floor32 = 1e-12; // squared residue at which the FP32 multi-shift phase hands over to refinement
@@ -134,6 +146,13 @@ struct tms_ctx
   uint64_t launches = 0;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // pipelined host-buffer column solves: a copy stream, two source and two
+  // solution staging buffers, and the events that order them
+  cudaStream_t cstream = nullptr;
+  double* colbuf[4] = {nullptr, nullptr, nullptr, nullptr}; // in 0, in 1, out 0, out 1
+  size_t colbuf_bytes = 0;
+  cudaEvent_t colev[8] = {}; // in ready 0/1, in free 0/1, out ready 0/1, out free 0/1
 };
 
 namespace tms_int
@@ -205,13 +224,41 @@ namespace tms_int
 
   inline Reducer reducer(tms_ctx* c) { return Reducer{c->red_partial, c->red_counter, c->red_result}; }
 
+  constexpr size_t kHostRing = 64 << 10;
+
+  // dst[0..nwords) = src[..]; either side may be mapped host memory
+  static __global__ void word_copy_kernel(const unsigned* __restrict__ src, unsigned* __restrict__ dst, int nwords)
+  {
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = src[i];
+    __threadfence_system();
+  }
+
+  // host scalars -> device memory, in stream order (staged in the mapped ring;
+  // the ring is reused only after the stream has drained)
+  inline tms_status put_small(tms_ctx* ctx, void* dst, const void* src, size_t bytes)
+  {
+    const size_t need = (bytes + 15) & ~size_t(15);
+    if (bytes % 4 || need > kHostRing) return fail(ctx, TMS_ERR_BAD_ARG, "put_small: %zu bytes", bytes);
+    if (ctx->hring_off + need > kHostRing)
+      {
+        CU(cudaStreamSynchronize(ctx->stream));
+        ctx->hring_off = 0;
+      }
+    memcpy(ctx->hring + ctx->hring_off, src, bytes);
+    ++ctx->launches;
+    word_copy_kernel<<<1, 64, 0, ctx->stream>>>(reinterpret_cast<const unsigned*>(ctx->hring_d + ctx->hring_off),
+                                                static_cast<unsigned*>(dst), (int)(bytes / 4));
+    ctx->hring_off += need;
+    CU(cudaGetLastError());
+    return TMS_OK;
+  }
+
   inline tms_status set_params(tms_ctx* ctx, double kappa, double mu, int has_anis, double anis, int slot = 0)
   {
     if (!(kappa > 0.0) || !std::isfinite(kappa) || !std::isfinite(mu))
       return fail(ctx, TMS_ERR_BAD_ARG, "invalid kappa %g / mu %g", kappa, mu);
     OpParams h{kappa, mu, has_anis ? anis : 1.0};
-    CU(cudaMemcpyAsync(ctx->prm + slot, &h, sizeof h, cudaMemcpyHostToDevice, ctx->stream));
-    return TMS_OK;
+    return put_small(ctx, ctx->prm + slot, &h, sizeof h);
   }
 
   // ------------------------------------------------------------ hop launch
@@ -284,6 +331,10 @@ namespace tms_int
   }
 
   inline LinkT<LINK_F64_18> links64(tms_ctx* c) { return LinkT<LINK_F64_18>{c->U64, (int)c->g.Vh}; }
+  inline LinkT<LINK_F64_12> links64r(tms_ctx* c) { return LinkT<LINK_F64_12>{c->U64, (int)c->g.Vh}; }
+  // the FP64 residual recomputations of the mixed solvers may read the links as
+  // 12 reals when the conf is SU(3) to FP64 rounding
+  inline bool reliable_links12(const tms_ctx* c) { return c->reliable_links12 && c->su3_dev < 1e-13; }
   inline LinkT<LINK_F32_12> links32r(tms_ctx* c) { return LinkT<LINK_F32_12>{c->U32r, (int)c->g.Vh}; }
   inline LinkT<LINK_F32_18> links32f(tms_ctx* c) { return LinkT<LINK_F32_18>{c->U32f, (int)c->g.Vh}; }
   inline LinkT<LINK_I16_12> links16r(tms_ctx* c) { return LinkT<LINK_I16_12>{c->U16r, (int)c->g.Vh}; }
@@ -488,9 +539,11 @@ namespace tms_int
 
   inline double read_result(tms_ctx* ctx)
   {
-    cudaMemcpyAsync(ctx->red_h, ctx->red_result, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    ++ctx->launches;
+    word_copy_kernel<<<1, 64, 0, ctx->stream>>>(reinterpret_cast<const unsigned*>(ctx->red_result),
+                                                reinterpret_cast<unsigned*>(ctx->red_hd), 2);
     cudaStreamSynchronize(ctx->stream);
-    return *ctx->red_h;
+    return *static_cast<volatile double*>(ctx->red_h);
   }
 
   // the parity-p half of a full-lattice field
@@ -620,14 +673,14 @@ namespace tms_int
     launch_hop<PREC_F64, LINK_F64_18>(c, c->stream, 0, 2, in_e, in_o, links64(c), prm, e);
   }
 
-  inline tms_status push_state(tms_ctx* ctx)
-  {
-    CU(cudaMemcpyAsync(ctx->st, ctx->st_h, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
-    return TMS_OK;
-  }
+  static_assert(sizeof(CgState) % 4 == 0 && sizeof(OpParams) % 4 == 0, "scalar transfers copy 32-bit words");
+  inline tms_status push_state(tms_ctx* ctx) { return put_small(ctx, ctx->st, ctx->st_h, sizeof(CgState)); }
   inline tms_status pull_state(tms_ctx* ctx)
   {
-    CU(cudaMemcpyAsync(ctx->st_h, ctx->st, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+    ++ctx->launches;
+    word_copy_kernel<<<1, 64, 0, ctx->stream>>>(reinterpret_cast<const unsigned*>(ctx->st),
+                                                reinterpret_cast<unsigned*>(ctx->st_hd), (int)(sizeof(CgState) / 4));
+    CU(cudaGetLastError());
     CU(cudaStreamSynchronize(ctx->stream));
     return TMS_OK;
   }

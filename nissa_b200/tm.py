@@ -391,6 +391,30 @@ class Lattice:
             self._check(st, "inv_tmD_cg_eoprec_batched", sd, out)
         return out, sd
 
+    def inv_tmD_cg_eoprec_columns(self, kappa, mu, sources_lx, niter, residue, anis=None, precision="double",
+                                  out=None, raise_on_error=True):
+        """inv_tmD_cg_eoprec for several sources one after the other; with host
+        buffers the copies of the neighbouring columns overlap each solve.
+        Returns (sols, [stats])."""
+        shape = (self.V, 4, 3, 2)
+        nc = len(sources_lx)
+        sb = [_Buf(x, shape) for x in sources_lx]
+        if out is None:
+            out = [self._new_out(sources_lx[0], shape) for _ in range(nc)]
+        ob = [_Buf(o, shape, out=True) for o in out]
+        self._mode(*sb, *ob)
+        sp = (ctypes.c_void_p * nc)(*[b.ptr for b in sb])
+        op = (ctypes.c_void_p * nc)(*[b.ptr for b in ob])
+        stats = (_lib.Stats * nc)()
+        a = self._anis(anis)
+        st = self.lib.tms_cg_eoprec_columns(self.h, nc, ctypes.cast(op, ctypes.c_void_p),
+                                            ctypes.cast(sp, ctypes.c_void_p), kappa, a[0], a[1], mu, int(niter),
+                                            float(residue), PRECISION[precision], ctypes.cast(stats, ctypes.c_void_p))
+        sd = [x.as_dict() for x in stats]
+        if raise_on_error:
+            self._check(st, "inv_tmD_cg_eoprec_columns", sd, out)
+        return out, sd
+
     def batch_session(self, nslots: int, precision: str = "single", anis=None) -> BatchSession:
         return BatchSession(self, nslots, precision, anis)
 
