@@ -602,19 +602,22 @@ namespace
   // Eq. (8)-(11) of inv_tmD_cg_eoprec_native (cg_invert_tmD_eoprec.cpp:102-150) on
   // device fields: the source's parities in ex[0] (even) and ex[1] (odd), the
   // solution's in ex[2], ex[3].  The operator parameters must be set.
-  tms_status eo_full_solve(tms_ctx* ctx, int niter, double residue, int precision, tms_stats* stats)
+  // (the FP64 steps around a mixed-precision solve read the links as 12 reals
+  // when the conf is SU(3) to rounding; the FP64 solve reads all 18)
+  template <int LF>
+  tms_status eo_full_solve_t(tms_ctx* ctx, const LinkT<LF>& U, int niter, double residue, int precision,
+                             tms_stats* stats)
   {
     Field* f = ctx->f64;
     for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
     Field *eta = ctx->ex, *psi = ctx->ex + 2; // [0] even, [1] odd
     const int n = (int)ctx->g.Vh;
     auto V = [&](const Field& x) { return view<PREC_F64>(x); };
-    auto U = links64(ctx);
     // Eq. (8a): te = D_ee^-1 eta_e ; Eq. (8b): varphi = g5 (eta_o + hop(te)/2) -> f0
     ++ctx->launches;
     diag_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(eta[0]), V(f[5]), ctx->prm, 1.0, 1);
     EpiSrcPrep<PREC_F64> sp{{V(f[0]), V(f[0])}, {V(eta[1]), V(eta[1])}};
-    launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
+    launch_hop<PREC_F64, LF>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
     CU(cudaGetLastError());
     // Eq. (9)
     const tms_status st = cg_dispatch<EoOp>(ctx, precision, niter, residue, false, stats);
@@ -622,9 +625,16 @@ namespace
     // Eq. (10): psi_o = K(-mu) x ; Eq. (11): psi_e = D_ee^-1 (eta_e + hop(psi_o)/2)
     kern_op<PREC_F64>(ctx, U, f[1], f[5], psi[1], -1.0, ctx->prm);
     EpiReco<PREC_F64> rc{{V(psi[0]), V(psi[0])}, {V(eta[0]), V(eta[0])}, ctx->prm, 1.0};
-    launch_hop<PREC_F64, LINK_F64_18>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
+    launch_hop<PREC_F64, LF>(ctx, ctx->stream, 0, 1, psi[1], psi[1], U, ctx->prm, rc);
     CU(cudaGetLastError());
     return st;
+  }
+
+  tms_status eo_full_solve(tms_ctx* ctx, int niter, double residue, int precision, tms_stats* stats)
+  {
+    if (precision != TMS_PREC_DOUBLE && reliable_links12(ctx))
+      return eo_full_solve_t(ctx, links64r(ctx), niter, residue, precision, stats);
+    return eo_full_solve_t(ctx, links64(ctx), niter, residue, precision, stats);
   }
 }
 
@@ -642,23 +652,19 @@ namespace
     for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
     Field *eta = ctx->ex, *psi = ctx->ex + 2; // [0] even, [1] odd
     for (auto& e : ctx->ex) TRY(alloc_field(ctx, e, PREC_F64));
-    const int64_t Vh = ctx->g.Vh;
-    const int n = (int)Vh;
+    const int n = (int)ctx->g.Vh;
+    const int lxblocks = div_up(ctx->g.V, LXCOPY_THREADS);
     auto V = [&](const Field& x) { return view<PREC_F64>(x); };
     // split_lx_vector_into_eo_parts(source)
     ++ctx->launches;
-    aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo, V(eta[0]));
-    ++ctx->launches;
-    aos_to_soa_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, src, ctx->lx_of_eo + Vh, V(eta[1]));
+    lx_split_kernel<PREC_F64><<<lxblocks, LXCOPY_THREADS, 0, ctx->stream>>>(ctx->g, src, V(eta[0]), V(eta[1]));
     CU(cudaGetLastError());
     if (src_read) CU(cudaEventRecord(src_read, ctx->stream));
     const tms_status st = eo_full_solve(ctx, niter, residue, precision, stats);
     if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
     // paste_eo_parts_into_lx_vector
     ++ctx->launches;
-    soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[0]), ctx->lx_of_eo, dst);
-    ++ctx->launches;
-    soa_to_aos_kernel<PREC_F64><<<div_up(n, 256), 256, 0, ctx->stream>>>(n, V(psi[1]), ctx->lx_of_eo + Vh, dst);
+    lx_paste_kernel<PREC_F64><<<lxblocks, LXCOPY_THREADS, 0, ctx->stream>>>(ctx->g, V(psi[0]), V(psi[1]), dst);
     CU(cudaGetLastError());
     if (dst_ready) CU(cudaEventRecord(dst_ready, ctx->stream));
     // lx residual check (cg_invert_tmD_eoprec.cpp:192-212): |g5 Q sol - src|^2 / |src|^2

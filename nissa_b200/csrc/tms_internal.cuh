@@ -349,14 +349,14 @@ namespace tms_int
     const int lx = lx_of_eo[idx];
     const size_t row = (layout == TMS_LAYOUT_LX) ? (size_t)lx : (size_t)idx;
     const int t = lx / (g.LX * g.LY * g.LZ);
-    const double2* a = reinterpret_cast<const double2*>(src + row * 72);
+    const double* a = src + row * 72; // 8-byte accesses: the caller's buffer need not be 16-byte aligned
     for (int mu = 0; mu < 4; mu++)
       {
         const double sg = (unfold && mu == 0 && t == g.T - 1) ? g.bc_t : 1.0;
         for (int k = 0; k < 9; k++)
           {
-            const double2 w = a[mu * 9 + k];
-            U[((size_t)(p * 4 + mu) * 9 + k) * g.Vh + ieo] = make_double2(w.x * sg, w.y * sg);
+            const double wx = a[2 * (mu * 9 + k)], wy = a[2 * (mu * 9 + k) + 1];
+            U[((size_t)(p * 4 + mu) * 9 + k) * g.Vh + ieo] = make_double2(wx * sg, wy * sg);
           }
       }
   }

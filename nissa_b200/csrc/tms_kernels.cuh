@@ -1113,14 +1113,10 @@ namespace tms
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const size_t row = site_map ? (size_t)site_map[i] : (size_t)i;
-    const double2* a = reinterpret_cast<const double2*>(aos + row * 24);
+    const double* a = aos + row * 24; // 8-byte accesses: the caller's buffer need not be 16-byte aligned
     C<R> v[12];
 #pragma unroll
-    for (int c = 0; c < 12; c++)
-      {
-        const double2 w = a[c];
-        v[c] = {R(w.x), R(w.y)};
-      }
+    for (int c = 0; c < 12; c++) v[c] = {R(a[2 * c]), R(a[2 * c + 1])};
     out.store(i, v);
   }
 
@@ -1133,8 +1129,77 @@ namespace tms
     const size_t row = site_map ? (size_t)site_map[i] : (size_t)i;
     C<R> v[12];
     in.load(i, v);
-    double2* a = reinterpret_cast<double2*>(aos + row * 24);
+    double* a = aos + row * 24;
 #pragma unroll
-    for (int c = 0; c < 12; c++) a[c] = make_double2((double)v[c].re, (double)v[c].im);
+    for (int c = 0; c < 12; c++)
+      {
+        a[2 * c] = (double)v[c].re;
+        a[2 * c + 1] = (double)v[c].im;
+      }
+  }
+
+  // split_lx_vector_into_eo_parts / paste_eo_parts_into_lx_vector for whole
+  // lx spinors: a block takes LXCOPY_THREADS consecutive lx sites, the AoS side
+  // moves through shared memory as one contiguous run of doubles (coalesced,
+  // 8-byte accesses), the SoA side at e/o index lx/2 of the site's parity
+  // (the e/o numbering keeps lx order within a parity and LZ is even).
+  constexpr int LXCOPY_THREADS = 128;
+  constexpr int LXCOPY_PITCH = 25; // doubles per staged site (24 + 1 against bank conflicts)
+
+  __device__ __forceinline__ int lx_parity(const Lattice& g, unsigned lx)
+  {
+    const unsigned z = lx % (unsigned)g.LZ;
+    unsigned q = lx / (unsigned)g.LZ;
+    const unsigned y = q % (unsigned)g.LY;
+    q /= (unsigned)g.LY;
+    const unsigned x = q % (unsigned)g.LX;
+    const unsigned t = q / (unsigned)g.LX;
+    return (int)((t + x + y + z) & 1u);
+  }
+
+  template <int P>
+  __global__ void __launch_bounds__(LXCOPY_THREADS)
+    lx_split_kernel(Lattice g, const double* __restrict__ aos, SpinorT<P> ev, SpinorT<P> od)
+  {
+    using R = typename SpinorT<P>::R;
+    __shared__ double sh[LXCOPY_THREADS * LXCOPY_PITCH];
+    const int64_t base = (int64_t)blockIdx.x * LXCOPY_THREADS;
+    const int nsite = (int)min((int64_t)LXCOPY_THREADS, g.V - base);
+    const double* in = aos + base * 24;
+    for (int k = threadIdx.x; k < nsite * 24; k += LXCOPY_THREADS) sh[(k / 24) * LXCOPY_PITCH + k % 24] = in[k];
+    __syncthreads();
+    if ((int)threadIdx.x >= nsite) return;
+    const unsigned lx = (unsigned)(base + threadIdx.x);
+    const double* v = sh + threadIdx.x * LXCOPY_PITCH;
+    C<R> c[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) c[k] = {R(v[2 * k]), R(v[2 * k + 1])};
+    (lx_parity(g, lx) ? od : ev).store((int)(lx >> 1), c);
+  }
+
+  template <int P>
+  __global__ void __launch_bounds__(LXCOPY_THREADS)
+    lx_paste_kernel(Lattice g, SpinorT<P> ev, SpinorT<P> od, double* __restrict__ aos)
+  {
+    using R = typename SpinorT<P>::R;
+    __shared__ double sh[LXCOPY_THREADS * LXCOPY_PITCH];
+    const int64_t base = (int64_t)blockIdx.x * LXCOPY_THREADS;
+    const int nsite = (int)min((int64_t)LXCOPY_THREADS, g.V - base);
+    if ((int)threadIdx.x < nsite)
+      {
+        const unsigned lx = (unsigned)(base + threadIdx.x);
+        C<R> c[12];
+        (lx_parity(g, lx) ? od : ev).load((int)(lx >> 1), c);
+        double* v = sh + threadIdx.x * LXCOPY_PITCH;
+#pragma unroll
+        for (int k = 0; k < 12; k++)
+          {
+            v[2 * k] = (double)c[k].re;
+            v[2 * k + 1] = (double)c[k].im;
+          }
+      }
+    __syncthreads();
+    double* out = aos + base * 24;
+    for (int k = threadIdx.x; k < nsite * 24; k += LXCOPY_THREADS) out[k] = sh[(k / 24) * LXCOPY_PITCH + k % 24];
   }
 }

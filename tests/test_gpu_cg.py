@@ -174,3 +174,36 @@ def test_columns_equal_single_solves(cuda_device, golden_cg, mode):
         import ctypes
         st = lat.lib.tms_cg_eoprec_columns(lat.h, 0, None, None, kappa, 0, 1.0, mu, 100, 1e-20, 0, None)
         assert st == 3
+
+
+def test_device_buffers_need_only_8_byte_alignment(cuda_device, golden_cg):
+    """Device pointers need only the alignment of a double: a conf, an operator
+    input/output and a full solve on buffers offset by one double give the same
+    bits as on 16-byte aligned ones."""
+    import torch
+    g = golden_cg
+    T, L = int(g["T"]), int(g["L"])
+    V = T * L ** 3
+    kappa, mu = float(g["kappa"]), float(g["mu"])
+    conf = torch.from_numpy(wl.gauge_conf(T, L, float(g["eps"]), int(g["seed"])))
+
+    def offset(a):
+        big = torch.zeros(a.numel() + 1, dtype=torch.float64, device="cuda:0")
+        v = big[1:].view(a.shape)
+        v.copy_(a)
+        assert v.data_ptr() % 16 == 8
+        return v
+
+    src = torch.from_numpy(wl.random_spinor(V, 81))
+    x = torch.from_numpy(wl.random_spinor(V // 2, 82))
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf.to("cuda:0"))
+        hop = lat.tmn2Deo_or_tmn2Doe_eos(1, x.to("cuda:0"))
+        sol, _ = lat.inv_tmD_cg_eoprec(kappa, mu, src.to("cuda:0"), 100000, 1e-22, precision="half")
+    with Lattice(T, L) as lat:
+        lat.upload_conf(offset(conf))
+        hop_o = lat.tmn2Deo_or_tmn2Doe_eos(1, offset(x), out=offset(torch.zeros_like(x)))
+        out = offset(torch.zeros_like(src))
+        lat.inv_tmD_cg_eoprec(kappa, mu, offset(src), 100000, 1e-22, precision="half", out=out)
+        assert torch.equal(hop_o, hop)
+        assert torch.equal(out, sol)
