@@ -589,6 +589,7 @@ def run_configs(args):
     conf = wl.gauge_conf(T, L, 0.35, 1, device=dev)
     with Lattice(T, L) as lat:
         lat.upload_conf(conf)
+        lat.set_tuning("links_single", 0)  # the configuration's FP32 12-real links (the default at this volume)
         cols = [torch.from_numpy(wl.point_source(T, L, spin=k // 3, col=k % 3)).to(dev) for k in range(12)]
         mixed = [torch.empty_like(cols[0]) for _ in range(12)]
         fp64 = [torch.empty_like(cols[0]) for _ in range(12)]

@@ -278,11 +278,13 @@ uint64_t tms_launch_count(const tms_ctx *ctx);
  * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
  * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
  * dropped by this factor, 0 < delta < 1), "links_single" (0: the FP32-spinor inner solver reads FP32
- * 12-real links, 1 (default): 16-bit fixed-point 12-real links), "links_reliable" (1 (default): the FP64
+ * 12-real links, 1: 16-bit fixed-point 12-real links; default 1 when the FP32 links would exceed 64 MB), "links_reliable" (1 (default): the FP64
  * residual recomputations of the mixed solvers read the links as 12 reals, row 2 rebuilt, when the conf
  * is SU(3) to 1e-13; 0: always 18 reals), "mrhs_per_thread" (right-hand sides one thread of the
  * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2),
- * "batch_graph_iters" (CG iterations per batch-session graph block, 0: chosen by batch size).  Results do not depend on the launch shapes. */
+ * "batch_graph_iters" (CG iterations per batch-session graph block, 0: chosen by batch size),
+ * "stream_priority" (the context's stream is recreated with this CUDA stream priority, an integer in the
+ * device's range, lower first; contexts of small volumes sharing a GPU with large ones use it).  Results do not depend on the launch shapes. */
 tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);
 /* Time the e/o hopping kernel alone with CUDA events on the context's stream: nrep launches,
  * each preceded (untimed) by a 512 MiB write that flushes the L2 when flush=1.

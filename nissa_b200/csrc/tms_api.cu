@@ -95,6 +95,8 @@ tms_status tms_create4(tms_ctx** out, int T, int LX, int LY, int LZ, double bc_t
   ctx->g.stride = round_up(V / 2, 64);
   ctx->g.bc_t = bc_t;
   ctx->device = device;
+  // FP32 12-real links (48 B per link) while they stay L2-resident, 16-bit ones beyond
+  ctx->single_links16 = (V * 4 * 48 > (int64_t(64) << 20)) ? 1 : 0;
   auto cleanup = [&](tms_status s) {
     tms_destroy(ctx);
     return s;
@@ -435,6 +437,22 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
     {
       if (!(value >= 1e-20 && value < 1.0)) return fail(ctx, TMS_ERR_BAD_ARG, "cgm_floor_single: in [1e-20, 1)");
       ctx->cgm_floor32 = value;
+      return TMS_OK;
+    }
+  if (k == "stream_priority")
+    {
+      // the context's stream is recreated with this priority (CUDA's convention:
+      // lower numbers run first); captured graphs run at the priority of the stream
+      int least = 0, greatest = 0;
+      CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      const int v = (int)value;
+      if ((double)v != value || v > least || v < greatest)
+        return fail(ctx, TMS_ERR_BAD_ARG, "stream_priority: an integer in [%d, %d]", greatest, least);
+      CU(cudaStreamSynchronize(ctx->stream));
+      cudaStream_t s = nullptr;
+      CU(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, v));
+      cudaStreamDestroy(ctx->stream);
+      ctx->stream = s;
       return TMS_OK;
     }
   if (k == "pdl")

@@ -161,16 +161,22 @@ class GpuResidency:
     and a source maker per volume, plus the free-HBM probe."""
 
     def __init__(self, volumes: dict, nslots: int = 16, precision: str = "single", device: int = 0,
-                 bc_t: float = -1.0):
+                 bc_t: float = -1.0, priorities: bool = False):
         import torch
         from .tm import Lattice
         self.torch = torch
         self.device = device
         self.lattices, self.sessions, self.shapes = {}, {}, {}
         self.streams = {}
+        # with priorities, smaller volumes get higher stream priorities: their
+        # short kernels are scheduled ahead of the waves of a large volume's kernels
+        order = sorted(volumes, key=lambda n: volumes[n][0] * volumes[n][1] ** 3)
+        least, greatest = torch.cuda.Stream.priority_range()
         for name, (T, L, conf) in volumes.items():
             lat = Lattice(T, L, bc_t=bc_t, device=device)
             lat.upload_conf(conf)
+            if priorities:
+                lat.set_tuning("stream_priority", min(least, greatest + order.index(name)))
             self.lattices[name] = lat
             self.sessions[name] = lat.batch_session(nslots, precision)
             self.shapes[name] = (T * L ** 3, 4, 3, 2)

@@ -84,3 +84,19 @@ def test_autotune_on_device(cuda_device, tmp_path):
         assert tune.autotune(lat, "half", cache=cache)["cached"]
         sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-20, precision="half")
         assert st["true_rel_res2"] < 1e-20
+
+
+def test_stream_priority_keeps_results(cuda_device):
+    """The context's stream recreated at a raised priority: the same solve
+    gives the same bits; priorities outside the device's range are refused."""
+    conf = wl.gauge_conf(8, 4, 0.35, seed=91)
+    src = wl.random_spinor(8 * 4 ** 3, 92)
+    with Lattice(8, 4) as lat:
+        lat.upload_conf(conf)
+        ref, _ = lat.inv_tmD_cg_eoprec(0.16, 0.01, src, 100000, 1e-20, precision="half")
+        lat.set_tuning("stream_priority", -1)
+        sol, _ = lat.inv_tmD_cg_eoprec(0.16, 0.01, src, 100000, 1e-20, precision="half")
+        assert np.array_equal(sol, ref)
+        for bad in (1, -1000, -0.5):
+            with pytest.raises(TmError):
+                lat.set_tuning("stream_priority", bad)
