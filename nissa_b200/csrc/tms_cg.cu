@@ -57,27 +57,56 @@ namespace
       return TMS_OK;
     }
 
-    // `iters` CG iterations in precision P (x in PX): v 1 r, 2 p, 3 t1, 4 te
+    // the paired x update (record with paired = true) keeps the second direction here
+    static constexpr bool kPaired = true;
+    static Field& p2(tms_ctx* c) { return c->lo[5]; }
+
+    // `iters` CG iterations in precision P (x in PX): v 1 r, 2 p, 3 t1, 4 te.
+    // paired (iters even): iteration 2k reads its direction from p and writes
+    // the next into p2, iteration 2k+1 reads p2, writes p and adds both
+    // iterations' steps to x; a replay starts and ends with the direction in p.
     template <int P, int PX, int LF>
-    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters)
+    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters,
+                       bool paired = false)
     {
-      const Field &r = v[1], &p = v[2], &t1 = v[3], &te = v[4];
+      const Field &r = v[1], &t1 = v[3], &te = v[4];
       const int* stop = &c->st->stop;
       const OpParams* prm = c->prm;
+      const int n = nsites(c);
       for (int it = 0; it < iters; it++)
         {
+          const bool odd = paired && (it & 1);
+          const Field& p = odd ? p2(c) : v[2];         // this iteration's direction
+          const Field& pn = (paired && !odd) ? p2(c) : v[2]; // the next one
           EpiInvDiag<P> a1{{view<P>(te), view<P>(te)}, prm, -1.0};
           launch_hop<P, LF>(c, s, 0, 1, p, p, U, prm, a1, NoFin{}, stop);
           EpiKern<P, true> b1{{view<P>(t1), view<P>(t1)}, {view<P>(p), view<P>(p)}, prm, -1.0};
           launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b1, FinAlpha{c->st}, stop);
           EpiInvDiag<P> a2{{view<P>(te), view<P>(te)}, prm, +1.0};
           launch_hop<P, LF>(c, s, 0, 1, t1, t1, U, prm, a2, NoFin{}, stop);
-          EpiKernCgUpdate<P, PX> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), prm, c->st, +1.0};
-          launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
-          const int n = nsites(c);
+          if (!paired)
+            {
+              EpiKernCgUpdate<P, PX, 1> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), prm, c->st, +1.0};
+              launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+            }
+          else if (!odd)
+            {
+              EpiKernCgUpdate<P, PX, 0> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), prm, c->st, +1.0};
+              launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+            }
+          else
+            {
+              EpiKernCgUpdate<P, PX, 2> b2{view<P>(t1), view<P>(r),   view<P>(p),       view<PX>(x),
+                                           prm,          c->st,         +1.0,             view<P>(v[2])};
+              launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+            }
           ++c->launches;
-          launch_pdl(c, xpay_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
-                     (const CgState*)c->st, stop);
+          if (paired)
+            launch_pdl(c, xpay_to_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
+                       view<P>(pn), (const CgState*)c->st, stop);
+          else
+            launch_pdl(c, xpay_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
+                       (const CgState*)c->st, stop);
         }
     }
   };
@@ -85,6 +114,7 @@ namespace
   struct LxOp
   {
     static constexpr int slot0 = 3;
+    static constexpr bool kPaired = false;
     static constexpr int nlo = 5;
     static int stride(tms_ctx* c) { return 2 * c->g.stride; }
     static int nsites(tms_ctx* c) { return 2 * c->g.stride; }
@@ -120,7 +150,8 @@ namespace
     // `iters` CG iterations: t = Q(-mu) p reducing |t|^2 ; s = Q(+mu) t fused
     // with the x and r updates ; p = r + beta p.   v 1 r, 2 p, 3 t
     template <int P, int PX, int LF>
-    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters)
+    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters,
+                       bool = false)
     {
       const Field &r = v[1], &p = v[2], &t = v[3];
       const int* stop = &c->st->stop;
@@ -151,6 +182,7 @@ namespace
   struct ClovOp
   {
     static constexpr int slot0 = 8;
+    static constexpr bool kPaired = false;
     static constexpr int nlo = 6;
     static int stride(tms_ctx* c) { return c->g.stride; }
     static int nsites(tms_ctx* c) { return (int)c->g.Vh; }
@@ -189,7 +221,8 @@ namespace
     // `iters` CG iterations in precision P (x in PX): v 1 r, 2 p, 3 t1, 4 te.
     // (p, K(false)K(true) p) = |K(true) p|^2 is reduced in the second launch.
     template <int P, int PX, int LF>
-    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters)
+    static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters,
+                       bool = false)
     {
       const Field &r = v[1], &p = v[2], &t1 = v[3], &te = v[4];
       const int* stop = &c->st->stop;
@@ -381,12 +414,15 @@ namespace
         S.stop = STOP_RUN;
         TRY(push_state(ctx));
         Field v[5] = {Field{}, lo[1], lo[2], lo[3], lo[4]};
+        // x updated every other iteration (e/o operator, even replay length)
+        const bool paired = Op::kPaired && ctx->graph_iters % 2 == 0;
         TRY(capture(ctx, slot, [&](cudaStream_t cs) {
-          Op::template record<P, PX>(ctx, cs, U, v, xlo, ctx->graph_iters);
+          Op::template record<P, PX>(ctx, cs, U, v, xlo, ctx->graph_iters, paired);
         }));
         CU(cudaEventRecord(ctx->ev0, ctx->stream));
         for (;;)
           {
+            const int iter0 = S.iter;
             TRY(launch_graph(ctx, slot));
             TRY(pull_state(ctx));
             if (S.stop == STOP_RUN) continue;
@@ -395,6 +431,23 @@ namespace
                 st = fail(ctx, TMS_ERR_NAN, "nanned (iteration %d)", S.iter);
                 break;
               }
+            // a replay cut after an odd number of paired iterations leaves the last
+            // step (alpha p, direction in p) out of x; after an even number the
+            // direction to keep is in p2
+            bool dir_in_p2 = false;
+            if constexpr (Op::kPaired)
+              if (paired)
+                {
+                  if ((S.iter - iter0) & 1)
+                    {
+                      ++ctx->launches;
+                      axpby_kernel<PX, PX, P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+                        n, 1.0, view<PX>(xlo), S.alpha, view<P>(lo[2]), view<PX>(xlo));
+                      CU(cudaGetLastError());
+                    }
+                  else
+                    dir_in_p2 = true;
+                }
             // reliable update: x += x_lo (FP64), r = b - A x (FP64)
             ++ctx->launches;
             axpby_kernel<PREC_F64, PREC_F64, PX><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
@@ -419,6 +472,14 @@ namespace
             S.stop = STOP_RUN;
             TRY(push_state(ctx));
             ++ctx->launches;
+            if constexpr (Op::kPaired)
+              if (dir_in_p2)
+                {
+                  xpay_to_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(
+                    n, view<P>(lo[1]), view<P>(Op::p2(ctx)), view<P>(lo[2]), ctx->st, nullptr);
+                  CU(cudaGetLastError());
+                  continue;
+                }
             xpay_kernel<P><<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(n, view<P>(lo[1]),
                                                                                        view<P>(lo[2]), ctx->st,
                                                                                        nullptr);

@@ -390,6 +390,7 @@ namespace tms
     double rr_prev;    // |r|^2 of the previous iteration
     double pAp;        // (p, A p)
     double alpha;      // step length
+    double alpha_prev; // step length of the previous iteration (paired x updates)
     double beta;       // direction update
     double target;     // stop when rr < target (residue * |b|^2)
     double rel_trigger;// reliable update when rr < rel_trigger
@@ -414,6 +415,7 @@ namespace tms
           st->stop = STOP_BREAKDOWN;
           return;
         }
+      st->alpha_prev = st->alpha;
       st->alpha = st->rr / pAp;
     }
   };
@@ -439,8 +441,11 @@ namespace tms
   // Second half of K(+mu)K(-mu) fused with the CG update:
   //   s = K(+mu) t1 ;  x += alpha p ;  r -= alpha s ;  reduce |r|^2
   // (cg_invert_template_threaded.hpp:82-107).  x may be kept in a wider
-  // precision (PX) than the iterated vectors (P).
-  template <int P, int PX>
+  // precision (PX) than the iterated vectors (P).  XM selects the x update:
+  // 1 x += alpha p; 0 none; 2 x += alpha_prev pp + alpha p, where pp is the
+  // previous iteration's direction (x updated every other iteration: the
+  // paired form reads and writes x half as often).
+  template <int P, int PX, int XM = 1>
   struct EpiKernCgUpdate
   {
     static constexpr bool kReduce = true;
@@ -450,6 +455,7 @@ namespace tms
     const OpParams* prm;
     const CgState* st;
     double sgn;
+    SpinorT<P> pp;    // XM == 2: the previous direction
     __device__ __forceinline__ double operator()(int par, int ieo, C<typename SpinorT<P>::R> acc[12]) const
     {
       using R = typename SpinorT<P>::R;
@@ -474,9 +480,21 @@ namespace tms
           n2 += (double)v[c].re * v[c].re + (double)v[c].im * v[c].im;
         }
       r.store(ieo, v);
-      p.load(ieo, v);
+      if (XM == 0) return n2;
       C<RX> xv[12];
       x.load(ieo, xv);
+      if (XM == 2)
+        {
+          pp.load(ieo, v);
+          const RX ap = RX(st->alpha_prev);
+#pragma unroll
+          for (int c = 0; c < 12; c++)
+            {
+              xv[c].re += ap * RX(v[c].re);
+              xv[c].im += ap * RX(v[c].im);
+            }
+        }
+      p.load(ieo, v);
       const RX ax = RX(st->alpha);
 #pragma unroll
       for (int c = 0; c < 12; c++)
@@ -988,6 +1006,26 @@ namespace tms
 #pragma unroll
     for (int c = 0; c < 12; c++) b[c] = cadd(a[c], cscale(b[c], beta));
     p.store(i, b);
+  }
+
+  // pout = r + beta pin (the paired CG keeps two directions)
+  template <int P>
+  static __global__ void __launch_bounds__(BLAS_THREADS)
+    xpay_to_kernel(int n, SpinorT<P> r, SpinorT<P> pin, SpinorT<P> pout, const CgState* st,
+                   const int* __restrict__ stop)
+  {
+    using R = typename SpinorT<P>::R;
+    pdl_enter();
+    if (stop && *stop) return;
+    const int i = blockIdx.x * BLAS_THREADS + threadIdx.x;
+    if (i >= n) return;
+    const R beta = R(st->beta);
+    C<R> a[12], b[12];
+    r.load(i, a);
+    pin.load(i, b);
+#pragma unroll
+    for (int c = 0; c < 12; c++) b[c] = cadd(a[c], cscale(b[c], beta));
+    pout.store(i, b);
   }
 
   // generic: reduce |a|^2 (or Re(a,b)) over n sites

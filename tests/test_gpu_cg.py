@@ -207,3 +207,26 @@ def test_device_buffers_need_only_8_byte_alignment(cuda_device, golden_cg):
         lat.inv_tmD_cg_eoprec(kappa, mu, offset(src), 100000, 1e-22, precision="half", out=out)
         assert torch.equal(hop_o, hop)
         assert torch.equal(out, sol)
+
+
+@pytest.mark.parametrize("precision", ["single", "half"])
+def test_paired_x_updates_match_unpaired(cuda_device, precision):
+    """An even CUDA-graph length makes the mixed e/o solver add the steps to x
+    every other iteration (two directions kept, the pending step flushed when
+    a reliable update cuts a replay); an odd length keeps the per-iteration
+    update.  Both reach the target with the same iteration count, and their
+    solutions agree to the solver's accuracy."""
+    T, L = 16, 8
+    conf = wl.gauge_conf(T, L, 0.35, seed=61)
+    src = wl.random_spinor(T * L ** 3, 62)
+    sols, its = [], []
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        for gi in (8, 7, 2):
+            lat.set_tuning("graph_iters", gi)
+            sol, st = lat.inv_tmD_cg_eoprec(0.1610, 0.005, src, 100000, 1e-20, precision=precision)
+            assert st["reliable_updates"] >= 2 and st["lx_rel_res2"] < 1e-19
+            sols.append(sol)
+            its.append(st["iterations"])
+    assert max(its) - min(its) <= 1
+    assert rel(sols[0], sols[1]) < 1e-8 and rel(sols[2], sols[1]) < 1e-8
