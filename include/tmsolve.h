@@ -131,6 +131,13 @@ tms_status tms_cg_eoprec_square(tms_ctx *ctx, double *sol, const double *guess, 
  * Full solve D_tm sol = src on lx spinors via Eq. (8)-(11) of the e/o preconditioning. */
 tms_status tms_cg_eoprec(tms_ctx *ctx, double *sol_lx, const double *src_lx, double kappa, int has_anis,
                          double anis, double mu, int niter, double residue, int precision, tms_stats *stats);
+/* The same with the reference's optional guess_Koo (inv_tmD_cg_eoprec's second argument,
+ * cg_invert_tmD_eoprec.cpp:102-137): an odd-site e/o spinor (Vh rows) from which the Eq. (9) CG
+ * starts; NULL for none.  Read only (the reference writes the new Koo solution into its by-value
+ * copy of the guess, so its caller sees no change either). */
+tms_status tms_cg_eoprec_guess(tms_ctx *ctx, double *sol_lx, const double *guess_Koo, const double *src_lx,
+                               double kappa, int has_anis, double anis, double mu, int niter, double residue,
+                               int precision, tms_stats *stats);
 /* inv_tmD_cg_eoprec for ncols sources one after the other (the loop over the 12 spin-colour columns
  * of a propagator, projects/ib/prop.cpp:41-112, calls it once per column).  Each column is the same
  * solve as tms_cg_eoprec; with host pointers the copy of column k+1's source in and of column k-1's

@@ -58,6 +58,7 @@ SIGNATURES = {
     "tms_apply_tmQ2": (I, [P, D, I, D, D, P, P]),
     "tms_cg_eoprec_square": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cg_eoprec": (I, [P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
+    "tms_cg_eoprec_guess": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cg_tmQ2": (I, [P, P, P, P, D, I, D, D, I, D, I, ctypes.POINTER(Stats)]),
     "tms_cgm_tmQ2": (I, [P, P, P, D, I, D, P, I, I, P, I, P]),
     "tms_cg_eoprec_batched": (I, [P, I, P, P, D, I, D, P, I, P, I, P]),

@@ -667,7 +667,7 @@ namespace
   // when the conf is SU(3) to rounding; the FP64 solve reads all 18)
   template <int LF>
   tms_status eo_full_solve_t(tms_ctx* ctx, const LinkT<LF>& U, int niter, double residue, int precision,
-                             tms_stats* stats)
+                             tms_stats* stats, const double* guess_Koo)
   {
     Field* f = ctx->f64;
     for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
@@ -680,8 +680,9 @@ namespace
     EpiSrcPrep<PREC_F64> sp{{V(f[0]), V(f[0])}, {V(eta[1]), V(eta[1])}};
     launch_hop<PREC_F64, LF>(ctx, ctx->stream, 1, 1, f[5], f[5], U, ctx->prm, sp);
     CU(cudaGetLastError());
-    // Eq. (9)
-    const tms_status st = cg_dispatch<EoOp>(ctx, precision, niter, residue, false, stats);
+    // Eq. (9), from the caller's odd-site guess when given
+    if (guess_Koo) TRY(spinor_in(ctx, guess_Koo, nullptr, ctx->g.Vh, f[1]));
+    const tms_status st = cg_dispatch<EoOp>(ctx, precision, niter, residue, guess_Koo != nullptr, stats);
     if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
     // Eq. (10): psi_o = K(-mu) x ; Eq. (11): psi_e = D_ee^-1 (eta_e + hop(psi_o)/2)
     kern_op<PREC_F64>(ctx, U, f[1], f[5], psi[1], -1.0, ctx->prm);
@@ -691,11 +692,12 @@ namespace
     return st;
   }
 
-  tms_status eo_full_solve(tms_ctx* ctx, int niter, double residue, int precision, tms_stats* stats)
+  tms_status eo_full_solve(tms_ctx* ctx, int niter, double residue, int precision, tms_stats* stats,
+                           const double* guess_Koo = nullptr)
   {
     if (precision != TMS_PREC_DOUBLE && reliable_links12(ctx))
-      return eo_full_solve_t(ctx, links64r(ctx), niter, residue, precision, stats);
-    return eo_full_solve_t(ctx, links64(ctx), niter, residue, precision, stats);
+      return eo_full_solve_t(ctx, links64r(ctx), niter, residue, precision, stats, guess_Koo);
+    return eo_full_solve_t(ctx, links64(ctx), niter, residue, precision, stats, guess_Koo);
   }
 }
 
@@ -707,7 +709,8 @@ namespace
   // given, `src_read` is recorded on the stream once the source has been read
   // and `dst_ready` once the solution is written.
   tms_status cg_eoprec_lx(tms_ctx* ctx, double* dst, const double* src, int niter, double residue, int precision,
-                          tms_stats* stats, cudaEvent_t src_read, cudaEvent_t dst_ready)
+                          tms_stats* stats, cudaEvent_t src_read, cudaEvent_t dst_ready,
+                          const double* guess_Koo = nullptr)
   {
     Field* f = ctx->f64;
     for (int i = 0; i <= 7; i++) TRY(alloc_field(ctx, f[i], PREC_F64));
@@ -721,7 +724,7 @@ namespace
     lx_split_kernel<PREC_F64><<<lxblocks, LXCOPY_THREADS, 0, ctx->stream>>>(ctx->g, src, V(eta[0]), V(eta[1]));
     CU(cudaGetLastError());
     if (src_read) CU(cudaEventRecord(src_read, ctx->stream));
-    const tms_status st = eo_full_solve(ctx, niter, residue, precision, stats);
+    const tms_status st = eo_full_solve(ctx, niter, residue, precision, stats, guess_Koo);
     if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
     // paste_eo_parts_into_lx_vector
     ++ctx->launches;
@@ -813,6 +816,14 @@ extern "C" {
 tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, double kappa, int has_anis, double anis,
                          double mu, int niter, double residue, int precision, tms_stats* stats)
 {
+  return tms_cg_eoprec_guess(ctx, sol_lx, nullptr, src_lx, kappa, has_anis, anis, mu, niter, residue, precision,
+                             stats);
+}
+
+tms_status tms_cg_eoprec_guess(tms_ctx* ctx, double* sol_lx, const double* guess_Koo, const double* src_lx,
+                               double kappa, int has_anis, double anis, double mu, int niter, double residue,
+                               int precision, tms_stats* stats)
+{
   TRY(check_conf(ctx));
   if (!sol_lx || !src_lx || niter <= 0 || !(residue > 0)) return fail(ctx, TMS_ERR_BAD_ARG, "bad solver arguments");
   TRY(set_params(ctx, kappa, mu, has_anis, anis));
@@ -825,7 +836,7 @@ tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, dou
       CU(cudaMemcpyAsync(ctx->stage, src_lx, bytes, cudaMemcpyHostToDevice, ctx->stream));
       src = dst = ctx->stage; // the source is split before the solution is pasted
     }
-  const tms_status st = cg_eoprec_lx(ctx, dst, src, niter, residue, precision, stats, nullptr, nullptr);
+  const tms_status st = cg_eoprec_lx(ctx, dst, src, niter, residue, precision, stats, nullptr, nullptr, guess_Koo);
   if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
   if (ctx->ptr_mode == TMS_PTR_HOST) CU(cudaMemcpyAsync(sol_lx, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   TRY(finish(ctx));

@@ -521,17 +521,19 @@ class Lattice:
         return sol, stats.as_dict()
 
     def inv_tmD_cg_eoprec(self, kappa, mu, source_lx, niter, residue, anis=None, precision="double", out=None,
-                          raise_on_error=True):
-        """Full solve D_tm sol = source (lx spinors) via e/o preconditioning.  Returns (sol, stats)."""
+                          raise_on_error=True, guess_Koo=None):
+        """Full solve D_tm sol = source (lx spinors) via e/o preconditioning,
+        the Eq. (9) CG started from guess_Koo (odd sites) when given.  Returns (sol, stats)."""
         shape = (self.V, 4, 3, 2)
         s = _Buf(source_lx, shape)
         sol = self._new_out(source_lx, shape) if out is None else out
         o = _Buf(sol, shape, out=True)
-        self._mode(s, o)
+        g = _Buf(guess_Koo, (self.Vh, 4, 3, 2))
+        self._mode(s, o, g)
         stats = _lib.Stats()
         a = self._anis(anis)
-        st = self.lib.tms_cg_eoprec(self.h, o.ptr, s.ptr, kappa, a[0], a[1], mu, int(niter), float(residue),
-                                    PRECISION[precision], ctypes.byref(stats))
+        st = self.lib.tms_cg_eoprec_guess(self.h, o.ptr, g.ptr, s.ptr, kappa, a[0], a[1], mu, int(niter),
+                                          float(residue), PRECISION[precision], ctypes.byref(stats))
         if raise_on_error:
             self._check(st, "inv_tmD_cg_eoprec", stats.as_dict(), sol)
         return sol, stats.as_dict()

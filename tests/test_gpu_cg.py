@@ -230,3 +230,32 @@ def test_paired_x_updates_match_unpaired(cuda_device, precision):
             its.append(st["iterations"])
     assert max(its) - min(its) <= 1
     assert rel(sols[0], sols[1]) < 1e-8 and rel(sols[2], sols[1]) < 1e-8
+
+
+def test_full_solve_from_guess(cuda_device, golden_cg):
+    """inv_tmD_cg_eoprec's optional guess_Koo: the Eq. (9) CG started from the
+    exact Koo solution (the square solve of the oracle's Eq. 8 source) needs no
+    iteration in any precision, and a zero guess behaves as none."""
+    g = golden_cg
+    T, L = int(g["T"]), int(g["L"])
+    V, Vh = T * L ** 3, T * L ** 3 // 2
+    kappa, mu = float(g["kappa"]), float(g["mu"])
+    conf = wl.gauge_conf(T, L, float(g["eps"]), int(g["seed"]))
+    geo = oracle.Geom(T, L)
+    ceo = geo.split(wl.apply_time_bc(conf, T, L, -1.0))
+    src = wl.random_spinor(V, 71)
+    eta = geo.split(src.reshape(V, -1)).reshape(2, Vh, 4, 3, 2)
+    varphi = eta[1] + 0.5 * geo.hop(ceo, 1, geo.inv_tmDee(kappa, mu, eta[0])).reshape(Vh, 4, 3, 2)
+    varphi[:, 2:] *= -1.0
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        y, _ = lat.inv_tmDkern_eoprec_square_eos_cg(kappa, mu, np.ascontiguousarray(varphi), 100000, 1e-28)
+        ref, st0 = lat.inv_tmD_cg_eoprec(kappa, mu, src, 100000, 1e-22)
+        assert st0["iterations"] > 10
+        sol, st1 = lat.inv_tmD_cg_eoprec(kappa, mu, src, 100000, 1e-22, guess_Koo=y)
+        assert st1["iterations"] <= 1 and rel(sol, ref) < 1e-9
+        z, st2 = lat.inv_tmD_cg_eoprec(kappa, mu, src, 100000, 1e-22, guess_Koo=np.zeros((Vh, 4, 3, 2)))
+        assert abs(st2["iterations"] - st0["iterations"]) <= 1 and rel(z, ref) < 1e-10
+        for prec in ("single", "half"):
+            s, st = lat.inv_tmD_cg_eoprec(kappa, mu, src, 100000, 1e-20, precision=prec, guess_Koo=y)
+            assert st["iterations"] <= 1 and rel(s, ref) < 1e-8
