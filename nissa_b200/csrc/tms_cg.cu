@@ -182,7 +182,8 @@ namespace
   struct ClovOp
   {
     static constexpr int slot0 = 8;
-    static constexpr bool kPaired = false;
+    static constexpr bool kPaired = true;
+    static Field& p2(tms_ctx* c) { return c->lo[5]; }
     static constexpr int nlo = 6;
     static int stride(tms_ctx* c) { return c->g.stride; }
     static int nsites(tms_ctx* c) { return (int)c->g.Vh; }
@@ -220,28 +221,50 @@ namespace
 
     // `iters` CG iterations in precision P (x in PX): v 1 r, 2 p, 3 t1, 4 te.
     // (p, K(false)K(true) p) = |K(true) p|^2 is reduced in the second launch.
+    // paired: the two directions and every-other-iteration x update of EoOp.
     template <int P, int PX, int LF>
     static void record(tms_ctx* c, cudaStream_t s, const LinkT<LF>& U, Field* v, const Field& x, int iters,
-                       bool = false)
+                       bool paired = false)
     {
-      const Field &r = v[1], &p = v[2], &t1 = v[3], &te = v[4];
+      const Field &r = v[1], &t1 = v[3], &te = v[4];
       const int* stop = &c->st->stop;
       const OpParams* prm = c->prm;
       const ClovT<P> cl = clov<P>(c);
+      const int n = nsites(c);
       for (int it = 0; it < iters; it++)
         {
+          const bool odd = paired && (it & 1);
+          const Field& p = odd ? p2(c) : v[2];
+          const Field& pn = (paired && !odd) ? p2(c) : v[2];
           EpiInvClov<P> a1{{view<P>(te), view<P>(te)}, cl, 1};
           launch_hop<P, LF>(c, s, 0, 1, p, p, U, prm, a1, NoFin{}, stop);
           EpiClovKern<P, true> b1{{view<P>(t1), view<P>(t1)}, {view<P>(p), view<P>(p)}, cl, prm, 1};
           launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b1, FinAlpha{c->st}, stop);
           EpiInvClov<P> a2{{view<P>(te), view<P>(te)}, cl, 0};
           launch_hop<P, LF>(c, s, 0, 1, t1, t1, U, prm, a2, NoFin{}, stop);
-          EpiClovKernCgUpdate<P, PX> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), cl, prm, c->st};
-          launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
-          const int n = nsites(c);
+          if (!paired)
+            {
+              EpiClovKernCgUpdate<P, PX, 1> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), cl, prm, c->st};
+              launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+            }
+          else if (!odd)
+            {
+              EpiClovKernCgUpdate<P, PX, 0> b2{view<P>(t1), view<P>(r), view<P>(p), view<PX>(x), cl, prm, c->st};
+              launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+            }
+          else
+            {
+              EpiClovKernCgUpdate<P, PX, 2> b2{view<P>(t1), view<P>(r), view<P>(p),  view<PX>(x),
+                                               cl,           prm,         c->st,        view<P>(v[2])};
+              launch_hop<P, LF>(c, s, 1, 1, te, te, U, prm, b2, FinBeta{c->st}, stop);
+            }
           ++c->launches;
-          launch_pdl(c, xpay_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
-                     (const CgState*)c->st, stop);
+          if (paired)
+            launch_pdl(c, xpay_to_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
+                       view<P>(pn), (const CgState*)c->st, stop);
+          else
+            launch_pdl(c, xpay_kernel<P>, div_up(n, BLAS_THREADS), BLAS_THREADS, 0, s, n, view<P>(r), view<P>(p),
+                       (const CgState*)c->st, stop);
         }
     }
   };

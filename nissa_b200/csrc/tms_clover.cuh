@@ -159,7 +159,9 @@ namespace tms
 
   // the second K of the CG matrix fused with the CG update:
   //   s = K(dag=false) t1 ;  x += alpha p ;  r -= alpha s ;  reduce |r|^2
-  template <int P, int PX>
+  // XM selects the x update as in EpiKernCgUpdate: 1 x += alpha p; 0 none;
+  // 2 x += alpha_prev pp + alpha p (paired, every other iteration)
+  template <int P, int PX, int XM = 1>
   struct EpiClovKernCgUpdate
   {
     static constexpr bool kReduce = true;
@@ -168,6 +170,7 @@ namespace tms
     ClovT<P> cl;
     const OpParams* prm;
     const CgState* st;
+    SpinorT<P> pp; // XM == 2: the previous direction
     __device__ __forceinline__ double operator()(int par, int ieo, C<typename SpinorT<P>::R> acc[12]) const
     {
       using R = typename SpinorT<P>::R;
@@ -191,9 +194,21 @@ namespace tms
           n2 += (double)v[c].re * v[c].re + (double)v[c].im * v[c].im;
         }
       r.store(ieo, v);
-      p.load(ieo, v);
+      if (XM == 0) return n2;
       C<RX> xv[12];
       x.load(ieo, xv);
+      if (XM == 2)
+        {
+          pp.load(ieo, v);
+          const RX ap = RX(st->alpha_prev);
+#pragma unroll
+          for (int c = 0; c < 12; c++)
+            {
+              xv[c].re += ap * RX(v[c].re);
+              xv[c].im += ap * RX(v[c].im);
+            }
+        }
+      p.load(ieo, v);
       const RX ax = RX(st->alpha);
 #pragma unroll
       for (int c = 0; c < 12; c++)

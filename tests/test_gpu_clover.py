@@ -101,3 +101,25 @@ def test_clover_errors(cuda_device):
         lat.upload_conf(wl.gauge_conf(4, 4, 0.4, seed=58))  # a new conf voids the clover term
         with pytest.raises(TmError):
             lat.tmclovDkern_eoprec_square_eos(0.13, 0.01, x)
+
+
+@pytest.mark.parametrize("precision", ["single", "half"])
+def test_clover_paired_x_updates_match_unpaired(cuda_device, precision):
+    """The twisted-clover mixed solver with the every-other-iteration x update
+    (even graph length) and with the per-iteration one (odd length): same
+    iteration count, solutions equal to the solver's accuracy."""
+    T, L = 16, 8
+    kappa, mu, cSW = 0.136, 0.01, 1.5
+    src = wl.random_spinor(T * L ** 3 // 2, 65)
+    sols, its = [], []
+    with Lattice(T, L) as lat:
+        lat.upload_conf(wl.gauge_conf(T, L, 0.35, seed=64))
+        lat.clover_term(cSW)
+        for gi in (8, 7):
+            lat.set_tuning("graph_iters", gi)
+            sol, st = lat.inv_tmclovDkern_eoprec_square_eos_cg(kappa, mu, src, 100000, 1e-20, precision=precision)
+            assert st["true_rel_res2"] < 1e-20 and st["reliable_updates"] >= 2
+            sols.append(sol)
+            its.append(st["iterations"])
+    assert abs(its[0] - its[1]) <= 1
+    assert rel(sols[0], sols[1]) < 1e-8
