@@ -52,7 +52,7 @@ namespace
     int cap = 0;          // right-hand sides the buffers hold
     int lo_prec = -1;
     BField hi[7];         // FP64: 0 b, 1 x, 2 r, 3 t1, 4 te, 5 s, 6 spare
-    BField lo[5];         // inner: 1 r, 2 p, 3 t1, 4 te
+    BField lo[5];         // inner: 0 second direction (paired x updates), 1 r, 2 p, 3 t1, 4 te
     BField xlo;           // inner x accumulator (FP32 for FP16 inner)
     CgState *st = nullptr, *st_h = nullptr, *mask = nullptr, *mask_h = nullptr;
     BatchParams *bp = nullptr, *bp_h = nullptr;
@@ -306,7 +306,7 @@ namespace
             cudaGraphExecDestroy(g);
             g = nullptr;
           }
-    for (int i = 1; i <= 4; i++) TRY(alloc_bfield(ctx, w->lo[i], P, n));
+    for (int i = (P == PREC_F64) ? 1 : 0; i <= 4; i++) TRY(alloc_bfield(ctx, w->lo[i], P, n));
     TRY(alloc_bfield(ctx, w->xlo, PX, n));
     w->lo_prec = P;
     return TMS_OK;
@@ -332,7 +332,11 @@ namespace
     tms_ctx* ctx = b->ctx;
     BatchWork* w = b->w;
     const int slot = P, nrhs = b->nslots, n = (int)ctx->g.Vh;
-    const int iters = batch_block_iters(ctx, nrhs);
+    // mixed precision: x updated every other iteration (two directions, lo[2]
+    // and lo[0]), so a block has an even number of iterations
+    constexpr bool paired = (P != PREC_F64);
+    const int iters0 = batch_block_iters(ctx, nrhs);
+    const int iters = paired ? iters0 + (iters0 & 1) : iters0;
     if (w->graph[slot] && w->graph_nrhs[slot] == nrhs && w->graph_iters[slot] == iters) return TMS_OK;
     if (w->graph[slot])
       {
@@ -348,17 +352,39 @@ namespace
     const uint64_t before = ctx->launches;
     for (int it = 0; it < iters; it++)
       {
+        const bool odd = paired && (it & 1);
+        const BField& p = odd ? w->lo[0] : w->lo[2];               // this iteration's direction
+        const BField& pn = (paired && !odd) ? w->lo[0] : w->lo[2]; // the next one
         EpiBInvDiag<P> a1{bview<P>(w->lo[4]), -1.0};
-        launch_mrhs<P>(ctx, w, cs, 0, nrhs, w->lo[2], U, a1, NoFinB{}, w->st);
-        EpiBKern<P, true> b1{bview<P>(w->lo[3]), bview<P>(w->lo[2]), -1.0};
+        launch_mrhs<P>(ctx, w, cs, 0, nrhs, p, U, a1, NoFinB{}, w->st);
+        EpiBKern<P, true> b1{bview<P>(w->lo[3]), bview<P>(p), -1.0};
         launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b1, FinAlphaB{w->st}, w->st);
         EpiBInvDiag<P> a2{bview<P>(w->lo[4]), +1.0};
         launch_mrhs<P>(ctx, w, cs, 0, nrhs, w->lo[3], U, a2, NoFinB{}, w->st);
-        EpiBKernCgUpdate<P, PX> b2e{bview<P>(w->lo[3]), bview<P>(w->lo[1]), bview<P>(w->lo[2]), bview<PX>(w->xlo),
-                                    w->st, +1.0};
-        launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b2e, FinBetaB{w->st}, w->st);
+        if (!paired)
+          {
+            EpiBKernCgUpdate<P, PX, 1> b2e{bview<P>(w->lo[3]), bview<P>(w->lo[1]), bview<P>(p), bview<PX>(w->xlo),
+                                           w->st, +1.0};
+            launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b2e, FinBetaB{w->st}, w->st);
+          }
+        else if (!odd)
+          {
+            EpiBKernCgUpdate<P, PX, 0> b2e{bview<P>(w->lo[3]), bview<P>(w->lo[1]), bview<P>(p), bview<PX>(w->xlo),
+                                           w->st, +1.0};
+            launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b2e, FinBetaB{w->st}, w->st);
+          }
+        else
+          {
+            EpiBKernCgUpdate<P, PX, 2> b2e{bview<P>(w->lo[3]), bview<P>(w->lo[1]), bview<P>(p), bview<PX>(w->xlo),
+                                           w->st,              +1.0,               bview<P>(w->lo[2])};
+            launch_mrhs<P>(ctx, w, cs, 1, nrhs, w->lo[4], U, b2e, FinBetaB{w->st}, w->st);
+          }
         ++ctx->launches;
-        xpay_mrhs_kernel<P><<<bg, 256, 0, cs>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]), w->st, nullptr);
+        if (paired)
+          xpay_to_mrhs_kernel<P><<<bg, 256, 0, cs>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(p), bview<P>(p),
+                                                      bview<P>(pn), 0, w->st, nullptr);
+        else
+          xpay_mrhs_kernel<P><<<bg, 256, 0, cs>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]), w->st, nullptr);
       }
     w->nodes[slot] = ctx->launches - before;
     ctx->launches = before;
@@ -427,6 +453,8 @@ namespace
     const dim3 bg(blas_grid(ctx), nrhs);
     CgState* S = w->st_h;
     TRY(session_graph<P>(b, U));
+    std::vector<int> iter0(nrhs);
+    for (int k = 0; k < nrhs; k++) iter0[k] = S[k].iter;
     CU(cudaGraphLaunch(w->graph[slot], ctx->stream));
     ctx->launches += w->nodes[slot];
     CU(cudaMemcpyAsync(S, w->st, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, ctx->stream));
@@ -467,6 +495,15 @@ namespace
           }
         else
           {
+            // paired x updates: a block cut after an odd number of iterations
+            // leaves the last step alpha p (direction in lo[2]) out of x_lo; after
+            // an even number the direction to restart from is in lo[0] (dir 1)
+            for (int k = 0; k < nrhs; k++)
+              if (!w->mask_h[k].stop) S[k].dir = ((S[k].iter - iter0[k]) & 1) ? 0 : 1;
+            CU(cudaMemcpyAsync(w->st, S, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
+            ++ctx->launches;
+            xflush_mrhs_kernel<PX, P><<<bg, 256, 0, ctx->stream>>>(n, nrhs, bview<PX>(w->xlo), bview<P>(w->lo[2]),
+                                                                    w->st, w->mask);
             // x += x_lo ; x_lo = 0 ; r = b - A x   (FP64, masked)
             ctx->launches += 2;
             axpby_mrhs_kernel<PREC_F64, PREC_F64, PX><<<bg, 256, 0, ctx->stream>>>(
@@ -503,8 +540,9 @@ namespace
                   w->mask);
                 CU(cudaMemcpyAsync(w->st, S, sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, ctx->stream));
                 ++ctx->launches;
-                xpay_mrhs_kernel<P><<<bg, 256, 0, ctx->stream>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]), w->st,
-                                                                 w->mask);
+                xpay_to_mrhs_kernel<P><<<bg, 256, 0, ctx->stream>>>(n, nrhs, bview<P>(w->lo[1]), bview<P>(w->lo[2]),
+                                                                    bview<P>(w->lo[0]), bview<P>(w->lo[2]), 1, w->st,
+                                                                    w->mask);
               }
           }
       }

@@ -146,7 +146,7 @@ namespace tms
   };
 
   // s = K(+mu) t1 ; x += alpha p ; r -= alpha s ; reduce |r|^2 (per right-hand side)
-  template <int P, int PX>
+  template <int P, int PX, int XM = 1>
   struct EpiBKernCgUpdate
   {
     static constexpr bool kReduce = true;
@@ -154,6 +154,7 @@ namespace tms
     SpinorBatch<PX> x;
     const CgState* st;
     double sgn;
+    SpinorBatch<P> pp; // XM == 2: the previous direction
     __device__ __forceinline__ double operator()(int k, int ieo, const BatchParams& bp,
                                                  C<typename SpinorT<P>::R> acc[12]) const
     {
@@ -182,10 +183,22 @@ namespace tms
           n2 += (double)v[c].re * v[c].re + (double)v[c].im * v[c].im;
         }
       rk.store(ieo, v);
-      p.rhs(k).load(ieo, v);
+      if (XM == 0) return n2;
       const SpinorT<PX> xk = x.rhs(k);
       C<RX> xv[12];
       xk.load(ieo, xv);
+      if (XM == 2)
+        {
+          pp.rhs(k).load(ieo, v);
+          const RX ap = RX(st[k].alpha_prev);
+#pragma unroll
+          for (int c = 0; c < 12; c++)
+            {
+              xv[c].re += ap * RX(v[c].re);
+              xv[c].im += ap * RX(v[c].im);
+            }
+        }
+      p.rhs(k).load(ieo, v);
 #pragma unroll
       for (int c = 0; c < 12; c++)
         {
@@ -386,6 +399,59 @@ namespace tms
             w[c] = {RO(re), RO(im)};
           }
         ok.store(i, w);
+      }
+  }
+
+  // pout = r + beta pin per right-hand side; with sel, right-hand side k reads
+  // pin2 instead of pin when st[k].dir is set (the paired CG's restart)
+  template <int P>
+  __global__ void __launch_bounds__(256)
+    xpay_to_mrhs_kernel(int n, int nrhs, SpinorBatch<P> r, SpinorBatch<P> pin, SpinorBatch<P> pin2,
+                        SpinorBatch<P> pout, int sel, const CgState* __restrict__ st,
+                        const CgState* __restrict__ mask)
+  {
+    using R = typename SpinorT<P>::R;
+    const int k = blockIdx.y;
+    if (k >= nrhs || (mask ? mask[k].stop : st[k].stop)) return;
+    const R beta = R(st[k].beta);
+    const SpinorT<P> rk = r.rhs(k), ik = (sel && st[k].dir) ? pin2.rhs(k) : pin.rhs(k), ok = pout.rhs(k);
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+      {
+        C<R> a[12], b[12];
+        rk.load(i, a);
+        ik.load(i, b);
+#pragma unroll
+        for (int c = 0; c < 12; c++) b[c] = cadd(a[c], cscale(b[c], beta));
+        ok.store(i, b);
+      }
+  }
+
+  // the paired CG's pending step: x += alpha p for the right-hand sides
+  // (unmasked) whose block was cut after an odd number of iterations (dir 0)
+  template <int PX, int P>
+  __global__ void __launch_bounds__(256)
+    xflush_mrhs_kernel(int n, int nrhs, SpinorBatch<PX> x, SpinorBatch<P> p, const CgState* __restrict__ st,
+                       const CgState* __restrict__ mask)
+  {
+    using RX = typename SpinorT<PX>::R;
+    const int k = blockIdx.y;
+    if (k >= nrhs || mask[k].stop || st[k].dir) return;
+    const RX a = RX(st[k].alpha);
+    const SpinorT<PX> xk = x.rhs(k);
+    const SpinorT<P> pk = p.rhs(k);
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+      {
+        C<RX> u[12];
+        C<typename SpinorT<P>::R> v[12];
+        xk.load(i, u);
+        pk.load(i, v);
+#pragma unroll
+        for (int c = 0; c < 12; c++)
+          {
+            u[c].re += a * RX(v[c].re);
+            u[c].im += a * RX(v[c].im);
+          }
+        xk.store(i, u);
       }
   }
 

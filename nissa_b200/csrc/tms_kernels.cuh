@@ -398,7 +398,7 @@ namespace tms
     int iter;          // iterations done
     int niter_max;
     int stop;          // 0 running, 1 converged, 2 max iterations, 3 reliable update due, 4 breakdown
-    int pad;
+    int dir;           // paired batched CG: which buffer holds the direction after a cut (set by the host)
   };
 
   enum StopCode { STOP_RUN = 0, STOP_CONVERGED = 1, STOP_MAXITER = 2, STOP_RELIABLE = 3, STOP_BREAKDOWN = 4 };
