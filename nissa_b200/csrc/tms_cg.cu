@@ -36,18 +36,25 @@ namespace
                                     bool mixed = false)
     {
       Field &t1 = ctx->f64[4], &te = ctx->f64[5], &s = ctx->f64[6];
-      if (mixed && reliable_links12(ctx))
+      if (mixed)
         {
-          auto U = links64r(ctx);
-          kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
-          kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
+          // the mixed solvers' recomputation: K(+mu) fused with r = b - s and |r|^2
+          auto res = [&](const auto& U) {
+            kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
+            EpiInvDiag<PREC_F64> a{{view<PREC_F64>(te), view<PREC_F64>(te)}, ctx->prm, +1.0};
+            launch_hop<PREC_F64>(ctx, ctx->stream, 0, 1, t1, t1, U, ctx->prm, a);
+            EpiKernResidual<PREC_F64> e{view<PREC_F64>(r), view<PREC_F64>(t1), view<PREC_F64>(b), ctx->prm, +1.0};
+            launch_hop<PREC_F64>(ctx, ctx->stream, 1, 1, te, te, U, ctx->prm, e);
+          };
+          if (reliable_links12(ctx)) res(links64r(ctx));
+          else res(links64(ctx));
+          CU(cudaGetLastError());
+          *rr = read_result(ctx);
+          return TMS_OK;
         }
-      else
-        {
-          auto U = links64(ctx);
-          kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
-          kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
-        }
+      auto U = links64(ctx);
+      kern_op<PREC_F64>(ctx, U, x, te, t1, -1.0, ctx->prm);
+      kern_op<PREC_F64>(ctx, U, t1, te, s, +1.0, ctx->prm);
       const int n = nsites(ctx);
       ++ctx->launches;
       residual_kernel<<<div_up(n, BLAS_THREADS), BLAS_THREADS, 0, ctx->stream>>>(

@@ -306,6 +306,39 @@ namespace tms
     }
   };
 
+  // r = b - K x in the second half of K (the residual recomputation of the
+  // mixed solvers fused into the stencil): out = b - g5 ((1/2k + i s mu g5) x - hop/4),
+  // reducing |r|^2
+  template <int P>
+  struct EpiKernResidual
+  {
+    static constexpr bool kReduce = true;
+    SpinorT<P> out; // r
+    SpinorT<P> x;   // the operand of this K at the output site
+    SpinorT<P> b;
+    const OpParams* prm;
+    double sgn;
+    __device__ __forceinline__ double operator()(int, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      using R = typename SpinorT<P>::R;
+      const C<R> z = zdiag<R>(*prm, sgn);
+      C<R> xv[12], bv[12];
+      x.load(ieo, xv);
+      b.load(ieo, bv);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 12; c++)
+        {
+          const C<R> d = diag_apply(xv[c], z, c);
+          const C<R> q = cscale(acc[c], R(0.25));
+          acc[c] = csub(bv[c], (c < 6) ? csub(d, q) : csub(q, d));
+          n2 += (double)acc[c].re * acc[c].re + (double)acc[c].im * acc[c].im;
+        }
+      out.store(ieo, acc);
+      return n2;
+    }
+  };
+
   // varphi = g5 (eta_o + hop/2): Eq. (8b), cg_invert_tmD_eoprec.cpp:37-58
   template <int P>
   struct EpiSrcPrep
