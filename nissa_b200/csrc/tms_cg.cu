@@ -1077,8 +1077,10 @@ tms_status tms_cgm_tmQ2(tms_ctx* ctx, double* const* sols, const double* src_lx,
           int corrections = 0;
           while (rt >= residues[k] * b2 && corrections < 4)
             {
-              // each e/o solve to a hundredth of the remaining factor (squared residues)
-              const double rel = std::min(1e-2, std::max(1e-22, 1e-2 * residues[k] * b2 / rt));
+              // each e/o solve to a tenth of the remaining factor (squared residues):
+              // one correction per shift at 32^3x64 with the true residual a third
+              // of its target (a hundredth took 4 % longer; 0.3 needed a second one)
+              const double rel = std::min(1e-2, std::max(1e-22, 1e-1 * residues[k] * b2 / rt));
               for (int p = 0; p < 2; p++)
                 {
                   ++ctx->launches;
