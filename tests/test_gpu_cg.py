@@ -259,3 +259,20 @@ def test_full_solve_from_guess(cuda_device, golden_cg):
         for prec in ("single", "half"):
             s, st = lat.inv_tmD_cg_eoprec(kappa, mu, src, 100000, 1e-20, precision=prec, guess_Koo=y)
             assert st["iterations"] <= 1 and rel(s, ref) < 1e-8
+
+
+def test_columns_error_leaves_context_usable(cuda_device):
+    """A column whose source is zero stops tms_cg_eoprec_columns with the
+    reference's invalid-norm error (host buffers: no copy is left running),
+    and the context solves normally afterwards."""
+    T, L = 8, 4
+    V = T * L ** 3
+    srcs = [wl.random_spinor(V, 91), np.zeros((V, 4, 3, 2)), wl.random_spinor(V, 92)]
+    with Lattice(T, L) as lat:
+        lat.upload_conf(wl.gauge_conf(T, L, 0.35, seed=90))
+        with pytest.raises(TmError) as e:
+            lat.inv_tmD_cg_eoprec_columns(0.16, 0.01, srcs, 100000, 1e-20, precision="half")
+        assert e.value.status == 8
+        sols, sts = lat.inv_tmD_cg_eoprec_columns(0.16, 0.01, [srcs[0], srcs[2]], 100000, 1e-20, precision="half")
+        ref, _ = lat.inv_tmD_cg_eoprec(0.16, 0.01, srcs[2], 100000, 1e-20, precision="half")
+        assert np.array_equal(sols[1], ref) and all(s["status"] == 0 for s in sts)
