@@ -589,7 +589,7 @@ def run_configs(args):
     conf = wl.gauge_conf(T, L, 0.35, 1, device=dev)
     with Lattice(T, L) as lat:
         lat.upload_conf(conf)
-        lat.set_tuning("links_single", 0)  # the configuration's FP32 12-real links (the default at this volume)
+        lat.set_tuning("links_single", 0)  # the configuration's FP32 12-real links
         cols = [torch.from_numpy(wl.point_source(T, L, spin=k // 3, col=k % 3)).to(dev) for k in range(12)]
         mixed = [torch.empty_like(cols[0]) for _ in range(12)]
         fp64 = [torch.empty_like(cols[0]) for _ in range(12)]
@@ -599,6 +599,8 @@ def run_configs(args):
                     for k in range(12)]
         ms_m, st_m = timed(lambda: solve_all("single", mixed), 1)
         ms_d, st_d = timed(lambda: solve_all("double", fp64), 1)
+        lat.set_tuning("links_single", 1)  # the library's default: 16-bit 12-real links
+        ms_16, _ = timed(lambda: solve_all("single", [torch.empty_like(cols[0]) for _ in range(12)]), 1)
         errs = [float(torch.linalg.norm(mixed[k] - fp64[k]) / torch.linalg.norm(fp64[k])) for k in range(12)]
         ref_sol, ref_s = reference_full_solve(conf, T, L, 0.161, 0.005, cols[0].cpu().numpy(), 1e-20)
         err_ref = None if ref_sol is None else float(
@@ -606,6 +608,7 @@ def run_configs(args):
         res["16^3x32 mixed FP32 (12-real links), 12 point columns, 1e-10"] = {
             "gpu_mixed_ms_per_solve": ms_m / 12, "gpu_fp64_ms_per_solve": ms_d / 12,
             "mixed_speedup_vs_fp64": ms_d / ms_m,
+            "gpu_mixed_16bit_links_ms_per_solve": ms_16 / 12,
             "iterations_mixed": [s["iterations"] for s in st_m[-1]],
             "iterations_fp64": [s["iterations"] for s in st_d[-1]],
             "true_rel_res2_max": max(s["true_rel_res2"] for s in st_m[-1]),

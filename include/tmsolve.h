@@ -285,7 +285,7 @@ uint64_t tms_launch_count(const tms_ctx *ctx);
  * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
  * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
  * dropped by this factor, 0 < delta < 1), "links_single" (0: the FP32-spinor inner solver reads FP32
- * 12-real links, 1: 16-bit fixed-point 12-real links; default 1 when the FP32 links would exceed 64 MB), "links_reliable" (1 (default): the FP64
+ * 12-real links, 1 (default): 16-bit fixed-point 12-real links, as fast or faster from 8^3x16 to 32^3x64), "links_reliable" (1 (default): the FP64
  * residual recomputations of the mixed solvers read the links as 12 reals, row 2 rebuilt, when the conf
  * is SU(3) to 1e-13; 0: always 18 reals), "mrhs_per_thread" (right-hand sides one thread of the
  * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2),

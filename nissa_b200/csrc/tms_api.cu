@@ -95,8 +95,6 @@ tms_status tms_create4(tms_ctx** out, int T, int LX, int LY, int LZ, double bc_t
   ctx->g.stride = round_up(V / 2, 64);
   ctx->g.bc_t = bc_t;
   ctx->device = device;
-  // FP32 12-real links (48 B per link) while they stay L2-resident, 16-bit ones beyond
-  ctx->single_links16 = (V * 4 * 48 > (int64_t(64) << 20)) ? 1 : 0;
   auto cleanup = [&](tms_status s) {
     tms_destroy(ctx);
     return s;

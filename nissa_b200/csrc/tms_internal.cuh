@@ -131,8 +131,7 @@ struct tms_ctx
   // reliable-update trigger of the mixed solvers
   int hop_cfg[3] = {0, 1, 0};
   double delta_single = 1e-3, delta_half = 0.005;
-  int single_links16 = 1; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0);
-                          // set by volume at creation
+  int single_links16 = 1; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
   int reliable_links12 = 1; // FP64 residuals of the mixed solvers on 12-real FP64 links (when SU(3) to rounding)
   double su3_dev = 1.0;     // largest deviation of the resident links from SU(3) (unitarity, row 2)
   int mrhs_r = 1; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
