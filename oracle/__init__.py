@@ -46,9 +46,23 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
-def build_ref(ref_root: str = "/root/reference", jobs: int = 8) -> str | None:
+def reference_root() -> str:
+    """The reference checkout: $NISSA_REFERENCE, else the default of the build
+    recipe (oracle/ref_build/Makefile, the one file that names it)."""
+    env = os.environ.get("NISSA_REFERENCE")
+    if env:
+        return env
+    try:
+        return subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref_build"), "print-ref"], capture_output=True,
+                              text=True, check=True).stdout.strip()
+    except Exception:
+        return ""
+
+
+def build_ref(ref_root: str | None = None, jobs: int = 8) -> str | None:
     """Build the reference's own code into oracle/_ref/nissa_ref (needs the reference tree)."""
-    if not os.path.isdir(os.path.join(ref_root, "src")):
+    ref_root = ref_root or reference_root()
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "src")):
         return REF_BIN if os.path.exists(REF_BIN) else None
     subprocess.check_call(["make", "-s", "-j%d" % jobs, "-C", os.path.join(HERE, "ref_build"), "REF=" + ref_root])
     return REF_BIN
@@ -307,7 +321,8 @@ def ref_available() -> bool:
     return os.path.exists(REF_BIN)
 
 
-def run_ref(op: str, T: int, L: int, arrays: dict, out_shape, threads: int | None = None, **params):
+def run_ref(op: str, T: int, L: int, arrays: dict, out_shape, threads: int | None = None, out_dtype=np.float64,
+            **params):
     """Run the reference's own code (oracle/_ref/nissa_ref) on raw arrays.
 
     ``arrays`` maps 'conf'/'in' to numpy arrays; returns (output array or None,
@@ -340,5 +355,22 @@ def run_ref(op: str, T: int, L: int, arrays: dict, out_shape, threads: int | Non
             return None, rec, cp.stdout
         out = None
         if out_shape is not None and os.path.exists(out_path):
-            out = np.fromfile(out_path, np.float64).reshape(out_shape)
+            out = np.fromfile(out_path, out_dtype).reshape(out_shape)
         return out, rec, cp.stdout
+
+
+def ref_geometry(T: int, L: int) -> dict:
+    """The reference's own e/o tables (set_eo_geometry, geometry_eo.cpp:41-100)
+    as its build leaves them for a T x L^3 lattice on one rank, keyed like
+    Geom.tables(): parity, eo_of_lx, lx_of_eo, neighup_eo, neighdw_eo."""
+    V = T * L ** 3
+    Vh = V // 2
+    flat, _, _ = run_ref("geom", T, L, {}, (11 * V,), out_dtype=np.int32)
+    o = 0
+    out = {}
+    for k, shape in (("parity", (V,)), ("eo_of_lx", (V,)), ("lx_of_eo", (2, Vh)), ("neighup_eo", (2, Vh, 4)),
+                     ("neighdw_eo", (2, Vh, 4))):
+        n = int(np.prod(shape))
+        out[k] = flat[o:o + n].reshape(shape).copy()
+        o += n
+    return out

@@ -12,7 +12,10 @@
 //   eo spinor   : Vh x [spin=4][col=3][re,im], sites in loclx_of_loceo order (geometry_eo.cpp:66-77)
 //
 // Usage: nissa_ref <op> T=<T> L=<L> [key=value ...]
-//   ops: plaq conf=...                          global_plaquette_lx_conf        (su3_paths/plaquette.hpp:77-82)
+//   ops: geom out=...                           the e/o geometry tables of set_eo_geometry (geometry_eo.cpp:41-100):
+//                                                int32 loclx_parity[V], loceo_of_loclx[V], loclx_of_loceo[2][Vh],
+//                                                loceo_neighup[2][Vh][4], loceo_neighdw[2][Vh][4], one after the other
+//        plaq conf=...                          global_plaquette_lx_conf        (su3_paths/plaquette.hpp:77-82)
 //        ildg2raw ildg=... out=...               read_ildg_gauge_conf             (io/reader.hpp:75-99)
 //        hop conf in out par=P                   tmn2Deo_or_tmn2Doe_eos           (dirac_operator_tmD_eoprec_portable.hpp:33-169)
 //        kern conf in out kappa mu               tmDkern_eoprec_eos               (dirac_operator_tmD_eoprec_portable.cpp:36-51)
@@ -29,6 +32,10 @@
 //        clovcgfull conf in out cSW kappa mu niter residue
 //                                                inv_tmclovD_cg_eoprec            (cg_invert_tmclovD_eoprec.cpp:55-120)
 //   common keys: anis=<double> (default: none), reps=<n> (timed repetitions, default 1)
+//   cgfull also reports every repetition's own time ("seconds_each"); with
+//   point_cols=<n> it ignores `in` and solves, in repetition r, the point source
+//   at the origin of spin-colour column r mod n (spin = k/3, colour = k%3); the
+//   output is the last repetition's solution
 //   cg with sample_iters=N: a bounded sample of the solve.  The reference's CG
 //   runs exactly N iterations (niter=N, unreachable residue) plus its final
 //   true-residual application, then takes its own non-convergence path
@@ -145,6 +152,17 @@ namespace
     fclose(f);
   }
 
+  void write_ints(const std::string& path, const std::vector<int>& v)
+  {
+    FILE* f = fopen(path.c_str(), "wb");
+    if (!f || fwrite(v.data(), sizeof(int), v.size(), f) != v.size())
+      {
+	fprintf(stderr, "cannot write %s\n", path.c_str());
+	exit(3);
+      }
+    fclose(f);
+  }
+
   template <typename F>
   void fill(F& field, const std::vector<double>& v, size_t nsites, size_t ndeg)
   {
@@ -217,7 +235,23 @@ int main(int narg, char** arg_v)
   double t_per_rep = 0;
   std::string extra;
 
-  if (op == "ildg2raw")
+  if (op == "geom")
+    {
+      // the reference's own tables, as set_eo_geometry left them (one rank: no borders)
+      std::vector<int> v;
+      for (size_t i = 0; i < V; i++) v.push_back(loclx_parity[i]);
+      for (size_t i = 0; i < V; i++) v.push_back(loceo_of_loclx[i]);
+      for (int par = 0; par < 2; par++)
+	for (size_t i = 0; i < Vh; i++) v.push_back(loclx_of_loceo[par][i]);
+      for (int par = 0; par < 2; par++)
+	for (size_t i = 0; i < Vh; i++)
+	  for (int mu = 0; mu < 4; mu++) v.push_back(loceo_neighup[par][i][mu]);
+      for (int par = 0; par < 2; par++)
+	for (size_t i = 0; i < Vh; i++)
+	  for (int mu = 0; mu < 4; mu++) v.push_back(loceo_neighdw[par][i][mu]);
+      write_ints(arg("out"), v);
+    }
+  else if (op == "ildg2raw")
     {
       LxField<quad_su3> conf("conf", WITH_HALO);
       read_ildg_gauge_conf(conf, arg("ildg"));
@@ -306,7 +340,8 @@ int main(int narg, char** arg_v)
       else if (op == "tmQ" || op == "cgfull" || op == "cgm")
 	{
 	  LxField<spincolor> in("in", WITH_HALO);
-	  fill(in, read_file(arg("in"), V * 24), V, 24);
+	  const int point_cols = (int)argd("point_cols", "0");
+	  if (point_cols == 0) fill(in, read_file(arg("in"), V * 24), V, 24);
 	  const double kappa = argd("kappa");
 	  if (op == "tmQ")
 	    {
@@ -322,9 +357,25 @@ int main(int narg, char** arg_v)
 	      const double mu = argd("mu");
 	      LxField<spincolor> sol("sol", WITH_HALO);
 	      const double t0 = now();
+	      std::string each = "\"seconds_each\": [";
 	      for (int r = 0; r < reps; r++)
-		inv_tmD_cg_eoprec(sol, std::nullopt, conf_lx, kappa, anis, mu, (int)argd("niter"), argd("residue"), in);
+		{
+		  if (point_cols > 0)
+		    {
+		      // point source at the origin, spin-colour column r mod point_cols (spin = k / 3, colour = k % 3)
+		      std::vector<double> v(V * 24, 0.0);
+		      const int k = r % point_cols;
+		      v[(k / 3) * 6 + (k % 3) * 2] = 1.0;
+		      fill(in, v, V, 24);
+		    }
+		  const double tr = now();
+		  inv_tmD_cg_eoprec(sol, std::nullopt, conf_lx, kappa, anis, mu, (int)argd("niter"), argd("residue"), in);
+		  char buf[32];
+		  snprintf(buf, sizeof buf, "%s%.9g", r ? ", " : "", now() - tr);
+		  each += buf;
+		}
 	      t_per_rep = (now() - t0) / reps;
+	      extra = each + "], ";
 	      dump(sol, arg("out"), V, 24);
 	    }
 	  else

@@ -9,7 +9,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = "/root/reference"
+import oracle  # noqa: E402  (test infrastructure: the checker)
+
+REFERENCE = oracle.reference_root()
 
 
 def pytest_configure(config):
@@ -25,6 +27,15 @@ def rel(a, b):
 @pytest.fixture(scope="session")
 def golden_small():
     return dict(np.load(os.path.join(GOLDEN, "ref_T4L4.npz")))
+
+
+KAT_CONF = os.path.join(GOLDEN, "L4T8conf")  # the reference's test/data/L4T8conf, copied by make_golden.py
+KAT_PLAQUETTE = 0.6350055722288719          # test/nissa/src/plaquette_computation.cpp:7-8
+
+
+@pytest.fixture(scope="session")
+def golden_geom():
+    return dict(np.load(os.path.join(GOLDEN, "ref_geom.npz")))
 
 
 @pytest.fixture(scope="session")

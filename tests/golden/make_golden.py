@@ -2,13 +2,22 @@
 code (nissa, built by oracle/ref_build into oracle/_ref/nissa_ref) on seeded
 inputs.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference checkout>]
+
+(default checkout: $NISSA_REFERENCE, else the one oracle/ref_build/Makefile reads)
 
 Fixtures:
   ref_T4L4.npz      4^4 lattice: every operator on the path and the CG / full
                     solve / multi-shift solves, inputs included.
   ref_T4L4_clover.npz  4^4 twisted clover: clover term, inverse, Schur operator,
                     its square and the full e/o solve.
+  ref_geom.npz      the reference's own e/o geometry tables (loclx_parity,
+                    loceo_of_loclx, loclx_of_loceo, loceo_neighup/dw of
+                    set_eo_geometry, geometry_eo.cpp:41-100) for 4^4 and 8^3x16.
+  L4T8conf          the reference's own 4^3x8 ILDG test configuration
+                    (test/data/L4T8conf, copied unchanged); its known
+                    plaquette is 0.6350055722288719
+                    (test/nissa/src/plaquette_computation.cpp:7-8).
   ref_T16L8_cg.npz  8^3x16 lattice, the plain FP64 CG workload (kappa=0.16,
                     mu=0.01, eps=0.4, point source, |r|/|b| <= 1e-12): the
                     conf is regenerated from its seed, the fixture keeps the
@@ -88,6 +97,21 @@ def make_cg(path):
     print("wrote", path, "iters", iters_from(so, "Total cg iterations"), "plaq", prec["plaquette"])
 
 
+def make_geom(path):
+    out = {}
+    for T, L in ((4, 4), (16, 8)):
+        for k, v in oracle.ref_geometry(T, L).items():
+            out["T%dL%d_%s" % (T, L, k)] = v
+    np.savez_compressed(path, **out)
+    print("wrote", path, sorted(out))
+
+
+def copy_known_answer_conf(ref_root, path):
+    import shutil
+    shutil.copyfile(os.path.join(ref_root, "test", "data", "L4T8conf"), path)
+    print("copied", path, os.path.getsize(path), "bytes")
+
+
 def make_clover(path):
     """Twisted clover on 4^4: the clover term, its twisted inverse (every 8th
     site), the Schur operator for both dagger flags, its square, and the full
@@ -118,9 +142,19 @@ def make_clover(path):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None)
+    ap.add_argument("--only", default=None, help="comma-separated subset: small,cg,clover,geom,kat")
     a = ap.parse_args()
-    oracle.build_ref(a.ref)
-    make_small(os.path.join(HERE, "ref_T4L4.npz"))
-    make_cg(os.path.join(HERE, "ref_T16L8_cg.npz"))
-    make_clover(os.path.join(HERE, "ref_T4L4_clover.npz"))
+    ref_root = a.ref or oracle.reference_root()
+    oracle.build_ref(ref_root)
+    only = set(a.only.split(",")) if a.only else {"small", "cg", "clover", "geom", "kat"}
+    if "geom" in only:
+        make_geom(os.path.join(HERE, "ref_geom.npz"))
+    if "kat" in only:
+        copy_known_answer_conf(ref_root, os.path.join(HERE, "L4T8conf"))
+    if "small" in only:
+        make_small(os.path.join(HERE, "ref_T4L4.npz"))
+    if "cg" in only:
+        make_cg(os.path.join(HERE, "ref_T16L8_cg.npz"))
+    if "clover" in only:
+        make_clover(os.path.join(HERE, "ref_T4L4_clover.npz"))

@@ -2,8 +2,8 @@
 
 The writer is pinned by the reference's own reader (read_ildg_gauge_conf run
 by the reference build, oracle/_ref), the reader by files the reference reads
-identically and, where the reference tree is mounted, by its 4^3x8 fixture
-with the golden plaquette 0.6350055722288719
+identically and by its 4^3x8 fixture (committed under tests/golden) with the
+golden plaquette 0.6350055722288719
 (test/nissa/src/plaquette_computation.cpp:7-8).  The device plaquette is
 compared with the oracle's global_plaquette_lx_conf."""
 import os
@@ -14,7 +14,7 @@ import pytest
 import oracle
 from nissa_b200 import Lattice, TmError
 from nissa_b200 import workload as wl
-from conftest import REFERENCE
+from conftest import KAT_CONF, KAT_PLAQUETTE
 
 pytestmark = pytest.mark.gpu
 
@@ -66,9 +66,11 @@ def test_size_mismatch_and_missing_file(cuda_device, tmp_path):
         assert e.value.status == 3
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE, "test/data/L4T8conf")),
-                    reason="reference test data not mounted")
 def test_reference_fixture_golden_plaquette(cuda_device):
+    """The reference's own known answer: its 4^3x8 test configuration
+    (test/data/L4T8conf, committed as tests/golden/L4T8conf) read by the device
+    ILDG reader has plaquette 0.6350055722288719
+    (test/nissa/src/plaquette_computation.cpp:7-8)."""
     with Lattice(8, 4) as lat:
-        lat.load_ildg(os.path.join(REFERENCE, "test/data/L4T8conf"))
-        assert abs(lat.plaquette() - 0.6350055722288719) < 1e-14
+        lat.load_ildg(KAT_CONF)
+        assert abs(lat.plaquette() - KAT_PLAQUETTE) < 1e-14

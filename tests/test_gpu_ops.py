@@ -14,12 +14,37 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-14
 
 
-@pytest.mark.parametrize("T,L", [(4, 4), (16, 8), (8, 6), (12, 4)])
+GEOM_KEYS = ("parity", "eo_of_lx", "lx_of_eo", "neighup_eo", "neighdw_eo")
+
+
+@pytest.mark.parametrize("T,L", [(4, 4), (16, 8)])
+def test_geometry_tables_match_reference_dump(cuda_device, golden_geom, T, L):
+    """Device tables against the reference's own loclx_parity, loceo_of_loclx,
+    loclx_of_loceo and loceo_neighup/dw (geometry_eo.cpp:41-100), bit-exact."""
+    with Lattice(T, L) as lat:
+        mine = lat.geometry_tables()
+    for k in GEOM_KEYS:
+        assert np.array_equal(mine[k], golden_geom["T%dL%d_%s" % (T, L, k)]), k
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("T,L", [(64, 32), (12, 6)])
+def test_geometry_tables_match_live_reference(cuda_device, T, L):
+    """The same at the headline volume (and a non-power-of-two one), against a
+    live dump by the reference build."""
+    with Lattice(T, L) as lat:
+        mine = lat.geometry_tables()
+    ref = oracle.ref_geometry(T, L)
+    for k in GEOM_KEYS:
+        assert np.array_equal(mine[k], ref[k]), k
+
+
+@pytest.mark.parametrize("T,L", [(8, 6), (12, 4)])
 def test_geometry_tables_bit_exact(cuda_device, T, L):
-    lat = Lattice(T, L)
-    mine = lat.geometry_tables()
+    with Lattice(T, L) as lat:
+        mine = lat.geometry_tables()
     ref = oracle.Geom(T, L).tables()
-    for k in ("parity", "eo_of_lx", "lx_of_eo", "neighup_eo", "neighdw_eo"):
+    for k in GEOM_KEYS:
         assert np.array_equal(mine[k], ref[k]), k
 
 

@@ -9,7 +9,7 @@ import pytest
 
 import oracle
 from nissa_b200 import workload as wl
-from conftest import REFERENCE, rel
+from conftest import KAT_CONF, KAT_PLAQUETTE, rel
 
 TOL_OP = 1e-14
 
@@ -81,13 +81,12 @@ def _read_ildg_binary(path):
     raise ValueError("no ildg-binary-data record")
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE, "test/data/L4T8conf")),
-                    reason="reference test data not mounted")
 def test_plaquette_known_answer():
     """Golden plaquette 0.6350055722288719 of the reference's 4^3x8 fixture
-    (test/nissa/src/plaquette_computation.cpp:7-8).  ILDG stores sites with x
+    (test/data/L4T8conf, committed as tests/golden/L4T8conf;
+    test/nissa/src/plaquette_computation.cpp:7-8).  ILDG stores sites with x
     fastest and links in the order x,y,z,t (io/reader.hpp:75-99 reorders)."""
-    raw = _read_ildg_binary(os.path.join(REFERENCE, "test/data/L4T8conf"))
+    raw = _read_ildg_binary(KAT_CONF)
     T, L = 8, 4
     ildg = raw.reshape(T, L, L, L, 4, 3, 3, 2)  # [t][z][y][x][mu_ildg=x,y,z,t]
     conf = np.empty((T, L, L, L, 4, 3, 3, 2))   # [t][x][y][z][mu=t,x,y,z]
@@ -97,7 +96,16 @@ def test_plaquette_known_answer():
     conf[..., 2, :, :, :] = lx[..., 1, :, :, :]
     conf[..., 3, :, :, :] = lx[..., 2, :, :, :]
     plaq = oracle.Geom(T, L).plaquette(conf.reshape(-1, 4, 3, 3, 2))
-    assert abs(plaq - 0.6350055722288719) / 0.6350055722288719 < 1e-14
+    assert abs(plaq - KAT_PLAQUETTE) / KAT_PLAQUETTE < 1e-14
+
+
+@pytest.mark.parametrize("T,L", [(4, 4), (16, 8)])
+def test_geometry_tables_match_reference(golden_geom, T, L):
+    """The oracle's tables equal the reference's own (set_eo_geometry,
+    geometry_eo.cpp:41-100), dumped by its build into ref_geom.npz."""
+    mine = oracle.Geom(T, L).tables()
+    for k in ("parity", "eo_of_lx", "lx_of_eo", "neighup_eo", "neighdw_eo"):
+        assert np.array_equal(mine[k], golden_geom["T%dL%d_%s" % (T, L, k)]), k
 
 
 def test_unit_conf_plaquette_and_free_hop():
