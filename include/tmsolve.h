@@ -276,12 +276,21 @@ tms_status tms_conf_plaquette(tms_ctx *ctx, int with_bc, double *plaquette);
 
 /* Number of CUDA kernels this context has launched (CUDA-graph replays count their nodes). */
 uint64_t tms_launch_count(const tms_ctx *ctx);
+/* Tiles of the staged hopping kernel (launch shape 7) whose bounded wait for their shared-memory
+ * copies gave up (their outputs are not written): 0 unless the memory system failed to deliver a
+ * copy; -1 on a CUDA error.  Waits for the context's stream. */
+int64_t tms_hop_stage_timeouts(tms_ctx *ctx);
 /* Tuning knobs (no reference counterpart), used by the autotuner: "hop_cfg_double",
  * "hop_cfg_single", "hop_cfg_half" (hopping-kernel launch shape 0..2: one site per thread, 128 threads;
  * 128 threads with registers capped for 4 (FP64) / 8 resident blocks; 256 threads capped for 2 / 4;
  * single and half only, when T is a multiple of 4 (else shape 0 is used): 3 two sites (t, t+T/2) per
  * thread in packed FP32 arithmetic with the neighbours streamed through shared memory by cp.async,
- * 4 two sites per thread in packed FP32 arithmetic),
+ * 4 two sites per thread in packed FP32 arithmetic; for any T: 5 one site per thread with the two spin
+ * rows of each half spinor in the lanes of packed FP32 arithmetic, 6 the same with each thread's
+ * neighbour spinors and links streamed through its own shared-memory slots by cp.async, three (FP32
+ * spinors: two) directions ahead, 7 tiles of lattice rows whose neighbour faces and links are staged
+ * in shared memory by bulk asynchronous copies before the same arithmetic (LZ a multiple of 8 and
+ * 16-bit or FP32 12-real links, else shape 0 is used)),
  * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
  * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
  * dropped by this factor, 0 < delta < 1), "links_single" (0: the FP32-spinor inner solver reads FP32
@@ -325,9 +334,13 @@ tms_status tms_bench_hop_batched(tms_ctx *ctx, int precision, int nrhs, int nrep
  * It calls no cudaMalloc/cudaFree and no allocating library routine: its
  * scratch is one fixed device array of TMS_NOALLOC_MAX_SITES*768+256 bytes
  * (12 MiB) that every GPU loading this library holds until the process exits.
- * The first call on a device looks up that array's device address
- * (cudaGetSymbolAddress) with the device current; make that first call before
- * any stream capture.  All calls share the array: calls that overlap on the GPU
+ * The first call on a device is its set-up: with the device current it looks
+ * up that array's device address (cudaGetSymbolAddress), which under CUDA's
+ * default lazy module loading also loads the library's device code there and
+ * materialises the array; make that first call before any stream capture and
+ * outside any phase that must not see device memory appear.  The address is
+ * kept for the life of the process, so the entry point is not for use across a
+ * cudaDeviceReset.  All calls share the array: calls that overlap on the GPU
  * race and must be serialised by the caller.  Lattices larger than
  * TMS_NOALLOC_MAX_SITES are rejected with TMS_ERR_BAD_ARG; `err` (may be NULL)
  * receives a message of at most errlen bytes. */

@@ -69,6 +69,7 @@ SIGNATURES = {
     "tms_batch_collect": (I, [P, I, P, ctypes.POINTER(Stats)]),
     "tms_batch_close": (I, [P]),
     "tms_launch_count": (ctypes.c_uint64, [P]),
+    "tms_hop_stage_timeouts": (ctypes.c_int64, [P]),
     "tms_set_tuning": (I, [P, ctypes.c_char_p, D]),
     "tms_bench_hop": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),
     "tms_bench_hop_batched": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),

@@ -108,6 +108,7 @@ tms_status tms_create4(tms_ctx** out, int T, int LX, int LY, int LZ, double bc_t
       cudaMalloc(&ctx->red_partial, sizeof(double) * ctx->red_cap) != cudaSuccess ||
       cudaMalloc(&ctx->red_counter, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&ctx->red_result, sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&ctx->tma_timeouts, sizeof(unsigned)) != cudaSuccess ||
       cudaHostAlloc(&ctx->st_h, sizeof(CgState), cudaHostAllocMapped) != cudaSuccess ||
       cudaMalloc(&ctx->cgm, sizeof(CgmState)) != cudaSuccess ||
       cudaMallocHost(&ctx->cgm_h, sizeof(CgmState)) != cudaSuccess ||
@@ -119,6 +120,7 @@ tms_status tms_create4(tms_ctx** out, int T, int LX, int LY, int LZ, double bc_t
       cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->hring_d), ctx->hring, 0) != cudaSuccess)
     return cleanup(TMS_ERR_CUDA);
   cudaMemset(ctx->red_counter, 0, sizeof(unsigned));
+  cudaMemset(ctx->tma_timeouts, 0, sizeof(unsigned));
   cudaMemset(ctx->st, 0, sizeof(CgState));
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
@@ -175,6 +177,7 @@ tms_status tms_destroy(tms_ctx* ctx)
   fr(ctx->st);
   fr(ctx->red_partial);
   fr(ctx->red_counter);
+  fr(ctx->tma_timeouts);
   fr(ctx->red_result);
   fr(ctx->stage);
   for (double*& b : ctx->colbuf) fr(b);
@@ -399,6 +402,16 @@ tms_status tms_apply_tmQ2(tms_ctx* ctx, double kappa, int has_anis, double anis,
 }
 
 uint64_t tms_launch_count(const tms_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int64_t tms_hop_stage_timeouts(tms_ctx* ctx)
+{
+  if (!ctx) return -1;
+  unsigned v = 0;
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess ||
+      cudaMemcpy(&v, ctx->tma_timeouts, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  return (int64_t)v;
+}
 
 tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
 {

@@ -5,6 +5,8 @@
 #include "tmsolve.h"
 #include "tms_kernels.cuh"
 #include "tms_pipe.cuh"
+#include "tms_hop_sp.cuh"
+#include "tms_hop_tma.cuh"
 #include "tms_clover.cuh"
 
 #include <cmath>
@@ -69,6 +71,7 @@ struct tms_ctx
   double* red_partial = nullptr;
   unsigned* red_counter = nullptr;
   double* red_result = nullptr;
+  unsigned* tma_timeouts = nullptr; // timed-out tile waits of the staged hop (launch shape 7); stays 0
   double* red_h = nullptr;       // pinned
   int red_cap = 0;
   // Scalars cross between host and device through mapped page-locked memory
@@ -129,7 +132,7 @@ struct tms_ctx
 
   // tuning (tms_set_tuning): hopping-kernel launch shape per precision, the
   // reliable-update trigger of the mixed solvers
-  int hop_cfg[3] = {0, 1, 0};
+  int hop_cfg[3] = {0, 1, 6};
   double delta_single = 1e-3, delta_half = 0.005;
   int single_links16 = 1; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
   int reliable_links12 = 1; // FP64 residuals of the mixed solvers on 12-real FP64 links (when SU(3) to rounding)
@@ -289,7 +292,49 @@ namespace tms_int
     const int nsite = (int)(npar * c->g.Vh);
     ++c->launches;
     if constexpr (P != PREC_F64)
-      if (c->hop_cfg[P] >= HOP_CFGS && c->g.T % 4 == 0)
+      {
+        if (c->hop_cfg[P] == 5)
+          {
+            launch_pdl(c, hop_sp_kernel<P, LF, Epi, Fin>, div_up(nsite, HOP_SP_THREADS), HOP_SP_THREADS, 0, s, c->g,
+                       par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+            return;
+          }
+        if (c->hop_cfg[P] == 6)
+          {
+            constexpr int DIST = (P == PREC_F16) ? 3 : 2;
+            constexpr int MINB = (P == PREC_F16) ? 5 : 3;
+            constexpr int smem = SppFmt<P, LF>::template smem<DIST>();
+            auto k = hop_spp_kernel<P, LF, Epi, Fin, DIST, MINB>;
+            static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            (void)attr;
+            launch_pdl(c, k, div_up(nsite, SPP_THREADS), SPP_THREADS, smem, s, c->g, par_out, npar, in_e, in_o, U, prm,
+                       epi, reducer(c), fin, stop);
+            return;
+          }
+        if constexpr (LF == LINK_I16_12 || LF == LINK_F32_12)
+          if (c->hop_cfg[P] == 7)
+            {
+              const TmaGeom G = tma_geom(c->g, c->tma_timeouts);
+              const int ntiles = G.ns ? (int)(npar * c->g.Vh / G.ns) : 0;
+              if (G.ns && ntiles <= c->red_cap)
+                {
+                  const size_t smem = tma_smem_bytes<P, LF>(G.nc, G.ns);
+                  auto k = hop_tma_kernel<P, LF, Epi, Fin>;
+                  // the largest tile: at most HOP_TMA_THREADS sites and two halo rows of at most 64 sites
+                  static const cudaError_t a1 = cudaFuncSetAttribute(
+                    k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    (int)tma_smem_bytes<P, LF>(HOP_TMA_THREADS + 128, HOP_TMA_THREADS));
+                  static const cudaError_t a2 = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                  (void)a1;
+                  (void)a2;
+                  launch_pdl(c, k, ntiles, HOP_TMA_THREADS, smem, s, c->g, G, par_out, npar, in_e, in_o, U, prm, epi,
+                             reducer(c), fin, stop);
+                  return;
+                }
+            }
+      }
+    if constexpr (P != PREC_F64)
+      if ((c->hop_cfg[P] == 3 || c->hop_cfg[P] == 4) && c->g.T % 4 == 0)
         {
           const int n2 = nsite / 2;
           if (c->hop_cfg[P] == 4)

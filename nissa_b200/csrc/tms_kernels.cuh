@@ -225,16 +225,28 @@ namespace tms
   // Each epilogue consumes the accumulated hop of one site (parity p, index
   // ieo) and returns its contribution to the kernel's reduction (if any).
 
+  // (FP32 arithmetic: the factors in FP32, from correctly rounded reciprocals,
+  // instead of FP64 divisions in every thread)
   template <typename R>
   __device__ __forceinline__ C<R> zdiag(const OpParams& o, double sgn)
   {
-    return {R(1.0 / (2.0 * o.kappa)), R(sgn * o.mu)};
+    if constexpr (sizeof(R) == 4) return {__frcp_rn(2.0f * float(o.kappa)), float(sgn * o.mu)};
+    else return {R(1.0 / (2.0 * o.kappa)), R(sgn * o.mu)};
   }
   template <typename R>
   __device__ __forceinline__ C<R> zinvdiag(const OpParams& o, double sgn)
   {
-    const double a = 1.0 / (2.0 * o.kappa), b = sgn * o.mu, nrm = a * a + b * b;
-    return {R(+a / nrm), R(-b / nrm)};
+    if constexpr (sizeof(R) == 4)
+      {
+        const float a = __frcp_rn(2.0f * float(o.kappa)), b = float(sgn * o.mu);
+        const float inv = __frcp_rn(fmaf(a, a, b * b));
+        return {a * inv, -b * inv};
+      }
+    else
+      {
+        const double a = 1.0 / (2.0 * o.kappa), b = sgn * o.mu, nrm = a * a + b * b;
+        return {R(+a / nrm), R(-b / nrm)};
+      }
   }
   // (z on spins 0,1; conj(z) on spins 2,3): tmDee_or_oo_eos, ..._portable.hpp:171-195
   template <typename R>
@@ -771,8 +783,11 @@ namespace tms
     static constexpr int MINB = (CFG == 0) ? 1 : (CFG == 1) ? (P == PREC_F64 ? 4 : 8) : (P == PREC_F64 ? 2 : 4);
   };
   constexpr int HOP_CFGS = 3;      // launch shapes of the one-site kernel
-  constexpr int HOP_CFGS_ALL = 5;  // FP32 arithmetic, T % 4 == 0: 3 the two-site packed kernel with
-                                   // the cp.async pipeline, 4 the two-site packed kernel
+  constexpr int HOP_CFGS_ALL = 8;  // FP32 arithmetic: 3 the two-site packed kernel with the cp.async
+                                   // pipeline and 4 the two-site packed kernel (both T % 4 == 0), 5 one
+                                   // site per thread, spin rows packed, 6 the same with its gathers
+                                   // streamed through shared memory by cp.async (tms_hop_sp.cuh), 7 tiles
+                                   // of rows staged in shared memory by bulk copies (tms_hop_tma.cuh)
 
   template <int P, int LF, class Epi, class Fin, int CFG = 0>
   __global__ void __launch_bounds__(HopCfg<P, CFG>::NT, HopCfg<P, CFG>::MINB)

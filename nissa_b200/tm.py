@@ -289,6 +289,11 @@ class Lattice:
         """CUDA kernels launched by this lattice's context so far."""
         return int(self.lib.tms_launch_count(self.h))
 
+    @property
+    def hop_stage_timeouts(self) -> int:
+        """Tiles of the staged hop (launch shape 7) whose wait for their copies gave up (0 normally)."""
+        return int(self.lib.tms_hop_stage_timeouts(self.h))
+
     def set_tuning(self, key: str, value: float):
         """Set a tuning knob of the C ABI (see tms_set_tuning in include/tmsolve.h)."""
         self._check(self.lib.tms_set_tuning(self.h, key.encode(), float(value)), "tms_set_tuning")

@@ -4,7 +4,9 @@ The choices (all results-neutral: every choice computes the same operator and
 solver) are the tuning knobs of the C ABI (tms_set_tuning):
 
   hop_cfg_<precision>  launch shape of the e/o hopping kernel (one or two
-                       sites per thread, register caps, cp.async pipeline)
+                       sites per thread, register caps, packed FP32 spin rows,
+                       gathers streamed through shared memory by cp.async,
+                       row tiles staged by bulk copies)
   links_single         FP32 or 16-bit links under the FP32 inner solver
   mrhs_per_thread      right-hand sides per thread of the batched kernel
 
@@ -21,7 +23,7 @@ import json
 import os
 import threading
 
-HOP_SHAPES = {"double": (0, 1, 2), "single": (0, 1, 2, 3, 4), "half": (0, 1, 2, 3, 4)}
+HOP_SHAPES = {"double": (0, 1, 2), "single": (0, 1, 2, 3, 4, 5, 6, 7), "half": (0, 1, 2, 3, 4, 5, 6, 7)}
 MRHS_CHOICES = (1, 2, 4)
 
 _lock = threading.Lock()

@@ -3,7 +3,11 @@ solution: mixed-precision solves under each tuning choice must reach the
 target true residual, agree with the FP64 solve and take about as many
 iterations.  Shapes 3 and 4 select the two-sites-per-thread packed-FP32
 kernel, which pairs the sites t and t+T/2 (T a multiple of 4; other T fall
-back to the one-site kernel)."""
+back to the one-site kernel); shape 5 the one-site kernel with the two spin
+rows of each half spinor in packed-FP32 lanes, 6 the same with its gathers
+streamed through shared memory by cp.async, 7 row tiles staged in shared
+memory by bulk copies (LZ a multiple of 8).  The staged kernel's bounded
+waits must never give up."""
 import numpy as np
 import pytest
 
@@ -25,7 +29,7 @@ def _solve_all(lat, src, prec, settings):
     return out
 
 
-@pytest.mark.parametrize("T,L", [(16, 8), (8, 4), (6, 4)])
+@pytest.mark.parametrize("T,L", [(16, 8), (8, 4), (6, 4), (4, 16)])
 @pytest.mark.parametrize("precision", ["single", "half"])
 def test_hop_shapes_agree(cuda_device, T, L, precision):
     conf = wl.gauge_conf(T, L, 0.35, seed=31)
@@ -37,10 +41,11 @@ def test_hop_shapes_agree(cuda_device, T, L, precision):
         links = [0, 1] if precision == "single" else [0]
         for ls in links:
             lat.set_tuning("links_single", ls)
-            for key_, val, sol, st in _solve_all(lat, src, precision, [(key, v) for v in range(5)]):
+            for key_, val, sol, st in _solve_all(lat, src, precision, [(key, v) for v in range(8)]):
                 assert st["true_rel_res2"] < 1e-20, (ls, val, st)
                 assert rel(sol, ref) < 1e-8, (ls, val)
                 assert st["iterations"] <= 1.1 * st0["iterations"] + 5, (ls, val, st["iterations"], st0["iterations"])
+        assert lat.hop_stage_timeouts == 0
 
 
 def test_full_lattice_packed(cuda_device):
@@ -52,7 +57,7 @@ def test_full_lattice_packed(cuda_device):
         lat.upload_conf(conf)
         ref, _ = lat.inv_tmQ2_cg(KAPPA, MU, src, 100000, 1e-22)
         for prec in ("single", "half"):
-            for v in (0, 3, 4):
+            for v in (0, 3, 4, 5, 6, 7):
                 lat.set_tuning("hop_cfg_" + prec, v)
                 sol, st = lat.inv_tmQ2_cg(KAPPA, MU, src, 100000, 1e-20, precision=prec)
                 assert rel(sol, ref) < 1e-8, (prec, v)
@@ -63,8 +68,9 @@ def test_shape_range_checked(cuda_device):
         with pytest.raises(TmError):
             lat.set_tuning("hop_cfg_double", 3)
         with pytest.raises(TmError):
-            lat.set_tuning("hop_cfg_single", 5)
+            lat.set_tuning("hop_cfg_single", 8)
         lat.set_tuning("hop_cfg_half", 4)
+        lat.set_tuning("hop_cfg_half", 7)
 
 
 def test_autotune_on_device(cuda_device, tmp_path):
