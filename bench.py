@@ -19,8 +19,17 @@ columns' solves);
 roofline = the inner solver's hopping kernel (hop + inverse diagonal, the first
 half of K) timed alone with CUDA events, L2 flushed between launches; fp64 = the
 plain FP64 GPU CG on the same solves and the FP64 e/o Dslash bandwidth;
-variants = the other inner precisions on the same solves; cpu_baseline = the
-reference's own OpenMP CG (oracle/_ref) on a bounded sample of the same solve.
+variants = the other inner precisions on the same solves; cpu_baseline = one
+whole solve of the reference's own OpenMP code (oracle/_ref) on the same conf,
+whose solution is also the yardstick of accuracy.rel_err_vs_reference.
+--impl reference times one whole reference solve per step.
+
+The same line carries, as sub-objects (rank 0, N = 1), the other
+configurations of the workload: configs_8c16 (plain FP64 CG, 8^3x16) and
+configs_16c32 (12 columns, FP32 inner with 12-real links, 16^3x32), each with
+the reference's own CPU solve timed and compared; batched_48 (48 right-hand
+sides at 24^3x48); cgm_32c64 (8-shift multi-mass CG, 3 sources, 32^3x64); serve
+(three resident volumes under Poisson load: p50/p99 latency at a stated rate).
 
 N > 1 GPUs run independent replicas (one gauge copy per GPU, each rank solving
 its own columns): the path needs no collective, scaling is weak.
@@ -48,9 +57,10 @@ PREC_DTYPE = {"double": "f64", "single": "f32 inner / f64 reliable updates",
               "half": "f16 storage, f32 arithmetic inner / f64 reliable updates"}
 METRIC = "CG solves/s & Dslash HBM GB/s, 32³×64 mixed vs FP64 @1e-10; p50/p99 serve"
 UNIT = "solves/s"
-CPU_SAMPLE_ITERS = 20
-HOP_KERNEL = {"half": "hop_kernel<FP16 spinors, 16-bit 12-real links> + inverse diagonal (first half of K)",
-              "single": "hop_kernel<FP32 spinors, 16-bit 12-real links> + inverse diagonal (first half of K)"}
+HOP_KERNEL = {"half": "hopping kernel of the FP16 inner solver (16-bit 12-real links) + inverse diagonal, "
+                      "the first half of K (the library's launch shape for FP16 spinors)",
+              "single": "hopping kernel of the FP32 inner solver (16-bit 12-real links) + inverse diagonal, "
+                        "the first half of K (the library's launch shape for FP32 spinors)"}
 # DRAM bytes of one launch of that kernel on this workload, from ncu
 HOP_TRAFFIC = {"half": 298.2e6}
 
@@ -121,30 +131,35 @@ def dist_setup():
     return ws, rank, local
 
 
-def cpu_reference_sample(conf_bc, T, L, kappa, mu, iters, threads):
-    """The reference's own CG (oracle/_ref) for `iters` iterations on the host:
-    seconds per iteration.  Falls back to the oracle restatement if the
-    reference build is absent."""
+def reference_solves(conf_bc, T, L, kappa, mu, residue, reps, threads):
+    """The reference's own full solve inv_tmD_cg_eoprec (oracle/_ref, its
+    unmodified OpenMP code) run `reps` times in one process on the host cores,
+    repetition r solving the point-source column r mod 12.  Returns (the last
+    repetition's solution, seconds of every repetition, threads, kind); falls
+    back to the oracle restatement (kind "port") when the reference build is
+    absent."""
     import oracle
-    Vh = T * L ** 3 // 2
-    src = np.random.default_rng(5).standard_normal((Vh, 4, 3, 2))
+    V = T * L ** 3
     if oracle.ref_available():
-        _, rec, _ = oracle.run_ref("cg", T, L, {"conf": conf_bc, "in": src}, None, kappa=kappa, mu=mu,
-                                   sample_iters=iters, threads=threads)
-        # the reference runs `iters` iterations plus one final residual operator application
-        return rec["seconds"] / (iters + 1), "reference", rec.get("threads", threads)
+        sol, rec, _ = oracle.run_ref("cgfull", T, L, {"conf": conf_bc}, (V, 4, 3, 2), kappa=kappa, mu=mu,
+                                     niter=100000, residue=residue, reps=reps, point_cols=12, threads=threads)
+        return sol, rec["seconds_each"], rec.get("threads", threads), "reference"
+    from nissa_b200 import workload as wl
     geo = oracle.Geom(T, L)
-    ceo = geo.split(conf_bc)
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    t0 = time.perf_counter()
-    geo.cg_eos(ceo, kappa, mu, src, iters, 1e-300)
-    return (time.perf_counter() - t0) / (iters + 1), "port", threads
+    secs, sol = [], None
+    for r in range(reps):
+        src = wl.point_source(T, L, spin=(r % 12) // 3, col=r % 3)
+        t0 = time.perf_counter()
+        sol, _, _ = geo.cg_full(conf_bc, kappa, mu, src, 100000, residue)
+        secs.append(time.perf_counter() - t0)
+    return sol, secs, threads, "port"
 
 
 def run_reference_arm(args):
-    """--impl reference: the reference's own OpenMP CG on the host cores, on a
-    bounded sample of each solve, scaled to solves/s by the FP64 iteration
-    count of the full solve."""
+    """--impl reference: the reference's own OpenMP full solve on the host
+    cores, one whole inv_tmD_cg_eoprec per step (FP64 to the same residue), on
+    the same conf, sources and parameters as the GPU arm."""
     ws, rank, _ = dist_setup()
     if rank != 0:
         return
@@ -153,22 +168,22 @@ def run_reference_arm(args):
     T, L = W["T"], W["L"]
     threads = os.cpu_count() or 1
     conf = wl.apply_time_bc(wl.gauge_conf(T, L, W["eps"], W["seed"]), T, L, W["bc_t"])
-    iters_full = args.fp64_iters
-    vals = []
-    for s in range(args.warmup + args.steps):
-        spi, kind, cores = cpu_reference_sample(conf, T, L, W["kappa"], W["mu"], CPU_SAMPLE_ITERS, threads)
-        if s >= args.warmup:
-            vals.append(1.0 / (spi * iters_full))
-    v = statistics.median(vals)
-    sample = ("inv_tmDkern_eoprec_square_eos_cg on %d^3x%d for %d iterations (+1 final residual) per step, "
-              "scaled by %d FP64 CG iterations per full solve" % (L, T, CPU_SAMPLE_ITERS, iters_full))
+    _, secs, cores, kind = reference_solves(conf, T, L, W["kappa"], W["mu"], W["residue"],
+                                            args.warmup + args.steps, threads)
+    timed = secs[args.warmup:]
+    v = len(timed) / sum(timed)
+    sample = ("%s inv_tmD_cg_eoprec on %d^3x%d, FP64 to |r|/|b| <= 1e-10, one whole solve per step (%d warm-up + "
+              "%d timed, point-source columns cycled as in the GPU arm), %.2f-%.2f s per solve"
+              % ("the reference's own" if kind == "reference" else "the oracle's restatement of", L, T, args.warmup,
+                 args.steps, min(timed), max(timed)))
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                      "data": "synthetic (seeded gauge recipe)",
+                      "data": "synthetic (seeded gauge recipe U=exp(i eps H), point sources)",
                       "config": {"workload": W["name"].split(", mixed")[0] + ", FP64 on the host cores, |r|/|b|<=1e-10",
                                  "T": T, "L": L, "kappa": W["kappa"], "mu": W["mu"], "eps": W["eps"],
-                                 "residue": W["residue"]},
+                                 "residue_sq": W["residue"], "sources": "12 point spin-colour columns at the origin, "
+                                                                     "cycled"},
                       "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
                       "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
           flush=True)
@@ -197,6 +212,8 @@ def run_ours(args):
     lat = Lattice(T, L, bc_t=W["bc_t"], device=local)
     lat.upload_conf(conf)
     assert lat.conf_is_su3
+    if args.hop_cfg >= 0:
+        lat.set_tuning("hop_cfg_" + args.precision, args.hop_cfg)
     plaquette = lat.plaquette()  # global_plaquette_lx_conf of the periodic links, on the device
 
     def column(k):
@@ -280,6 +297,7 @@ def run_ours(args):
         solve(k, out=sol)
         errs.append(float(torch.linalg.norm(sol - ref) / torch.linalg.norm(ref)))
     fp64_sec = statistics.mean(s["seconds"] for s in fp64_stats)
+    accuracy_vs_ref = {}
     mixed_sec = statistics.mean(s["seconds"] for s in stats)
 
     # --- the 12 columns as one batched solve (one pass over the links per operator step) ----
@@ -311,17 +329,25 @@ def run_ours(args):
                           "true_rel_res2_max": max(x["true_rel_res2"] for x in vs)}
     lat.set_tuning("links_single", 1)
 
-    # --- CPU baseline: the reference's own CG on a bounded sample (rank 0, N=1 only) ---------
+    # --- CPU baseline: one whole reference solve of column 0 (rank 0, N=1 only), and the -------
+    # --- headline solution's error against it -------------------------------------------------
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
             conf_bc = wl.apply_time_bc(conf, T, L, W["bc_t"])
-            spi, kind, cores = cpu_reference_sample(conf_bc, T, L, kappa, mu, CPU_SAMPLE_ITERS, os.cpu_count() or 1)
-            it64 = fp64_stats[0]["iterations"]
-            cpu = {"value": 1.0 / (spi * it64), "unit": UNIT, "cores": cores, "kind": kind,
-                   "sample": "reference inv_tmDkern_eoprec_square_eos_cg, %d iterations (+1 final residual) on the "
-                             "same 32^3x64 conf, %.3f s/iteration, scaled by the %d FP64 iterations of a full solve"
-                             % (CPU_SAMPLE_ITERS, spi, it64)}
+            ref_sol, secs, cores, kind = reference_solves(conf_bc, T, L, kappa, mu, residue, 1, os.cpu_count() or 1)
+            cpu = {"value": 1.0 / secs[0], "unit": UNIT, "cores": cores, "kind": kind,
+                   "sample": "%s inv_tmD_cg_eoprec, one whole FP64 solve of point column 0 on the same 32^3x64 conf "
+                             "to |r|/|b| <= 1e-10: %.2f s" % ("the reference's own" if kind == "reference" else
+                                                              "the oracle's restatement of", secs[0])}
+            ref_d = torch.from_numpy(ref_sol).to(dev)
+            solve(0, out=sol)
+            solve(0, precision="double", out=ref)
+            nref = torch.linalg.norm(ref_d)
+            accuracy_vs_ref = {"rel_err_vs_reference": float(torch.linalg.norm(sol - ref_d) / nref),
+                               "fp64_rel_err_vs_reference": float(torch.linalg.norm(ref - ref_d) / nref),
+                               "reference_column": 0, "reference_kind": kind}
+            del ref_d
             # the reference's FP64 e/o Dslash on the same conf (3 repetitions), same bytes model
             import oracle
             if oracle.ref_available():
@@ -337,6 +363,28 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank != 0:
         return
+
+    # --- the other configurations, as sub-objects of this line (rank 0, N=1) ---------------------
+    legs = {}
+    if ws == 1 and not args.no_legs:
+        lat.close()
+        del cols, sol, ref
+        torch.cuda.empty_cache()
+        for name, fn in (("configs", leg_configs), ("batched_48", leg_batched), ("cgm_32c64", leg_cgm),
+                         ("serve", leg_serve)):
+            t0 = time.perf_counter()
+            try:
+                r = fn(args)
+            except Exception as e:  # a leg is reported, never required for the headline
+                r = {"error": "%s: %s" % (type(e).__name__, e)}
+            if name == "configs" and "results" in r:
+                for k, v in r["results"].items():
+                    legs["configs_8c16" if k.startswith("8^3") else "configs_16c32"] = dict(v, config=k)
+            else:
+                legs[name] = r
+            log("leg %s: %.1f s" % (name, time.perf_counter() - t0))
+            torch.cuda.empty_cache()
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -361,7 +409,7 @@ def run_ours(args):
         "fp64": {"solves_per_s": 1.0 / fp64_sec, "iterations": fp64_stats[0]["iterations"],
                  "mixed_speedup_vs_fp64": fp64_sec / mixed_sec,
                  "dslash_gbs": d64_gbs, "dslash_frac": d64_gbs / peak, "dslash_ms": d64_ms},
-        "accuracy": {"mixed_rel_err_vs_fp64": max(errs),
+        "accuracy": {"mixed_rel_err_vs_fp64": max(errs), **accuracy_vs_ref,
                      "true_rel_res2_max": max(s["true_rel_res2"] for s in stats),
                      "lx_rel_res2_max": max(s["lx_rel_res2"] for s in stats)},
         "solver": {"iterations_mean": statistics.mean(s["iterations"] for s in stats),
@@ -370,6 +418,7 @@ def run_ours(args):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    line.update(legs)
     print(json.dumps(line), flush=True)
 
 
@@ -403,11 +452,11 @@ CGM_WORKLOAD = dict(name="tm Q^2 multi-shift CGM, 32^3x64, 8 masses log-spaced i
                     residue=1e-20, bc_t=-1.0)
 
 
-def run_cgm(args):
+def leg_cgm(args):
     """The multi-shift workload (one step = one source solved for all 8 masses:
     FP32 multi-shift to |r|/|b| ~ 1e-6, then per shift a defect correction
     through the mixed-precision e/o solver, every shift to |r|/|b| <= 1e-10
-    checked in FP64); reported as an extra line, not the headline."""
+    checked in FP64), against the FP64 multi-shift CG on the same sources."""
     import torch
     from nissa_b200 import Lattice
     from nissa_b200 import workload as wl
@@ -436,11 +485,11 @@ def run_cgm(args):
         res[prec] = {"sources_per_s": 3 / dt, "s_per_source": dt / 3,
                      "iterations": [s["iterations"] for s in stats[0]],
                      "true_rel_res2_max": max(x["true_rel_res2"] for st in stats for x in st)}
-    print(json.dumps({"workload": W["name"].replace("32^3x64", "%d^3x%d" % (L, T)), "kappa": W["kappa"],
-                      "masses": W["masses"], "residue_sq": W["residue"], "mixed": res[args.cgm_precision],
-                      "fp64": res["double"],
-                      "mixed_speedup_vs_fp64": res["double"]["s_per_source"] / res[args.cgm_precision]["s_per_source"]}),
-          flush=True)
+    lat.close()
+    return {"workload": W["name"].replace("32^3x64", "%d^3x%d" % (L, T)), "kappa": W["kappa"],
+            "masses": W["masses"], "residue_sq": W["residue"], "mixed": res[args.cgm_precision],
+            "fp64": res["double"],
+            "mixed_speedup_vs_fp64": res["double"]["s_per_source"] / res[args.cgm_precision]["s_per_source"]}
 
 
 BATCH_WORKLOAD = dict(name="48-RHS batched e/o CG, 24^3x48: 12 spin-colour-diluted Z2 sources x mu in "
@@ -449,13 +498,12 @@ BATCH_WORKLOAD = dict(name="48-RHS batched e/o CG, 24^3x48: 12 spin-colour-dilut
                       bc_t=-1.0)
 
 
-def run_batched(args):
+def leg_batched(args):
     """The batched workload: the 48 right-hand sides solved in one batched
     solve (one launch per operator step for all of them, CUDA graphs,
     autotuned kernel shapes) against the same 48 solved one at a time with
     the same precision; reports right-hand sides per second and the largest
-    difference between a batched and an alone solution (an extra line, not
-    the headline)."""
+    difference between a batched and an alone solution."""
     import torch
     from nissa_b200 import Lattice, tune
     from nissa_b200 import workload as wl
@@ -513,7 +561,8 @@ def run_batched(args):
     e1.record()
     torch.cuda.synchronize()
     ms_64 = e0.elapsed_time(e1) / n64
-    print(json.dumps({"workload": (W["name"] % PREC_NAME[prec]).replace("24^3x48", "%d^3x%d" % (L, T)),
+    lat.close()
+    return ({"workload": (W["name"] % PREC_NAME[prec]).replace("24^3x48", "%d^3x%d" % (L, T)),
                       "rhs": n, "precision": prec,
                       "batched": {"rhs_per_s": n / (ms_b * 1e-3), "ms": ms_b,
                                   "iterations_max": max(s["iterations"] for s in st_b),
@@ -526,10 +575,10 @@ def run_batched(args):
                       "batched_speedup": ms_1 / ms_b,
                       "batched_mixed_speedup_vs_fp64": ms_64 * n / ms_b,
                       "max_rel_diff_batched_vs_alone": diff,
-                      "tuning": {"batched": tuned_b, "single": tuned_1}, "clocks": clk.summary()}), flush=True)
+                      "tuning": {"batched": tuned_b, "single": tuned_1}, "clocks": clk.summary()})
 
 
-def run_configs(args):
+def leg_configs(args):
     """The two configurations below the headline volume, each with the
     reference's own CPU code timed on the same inputs (rank 0 host cores):
     (1) 8^3x16 plain FP64 e/o CG, kappa 0.16, mu 0.01, eps 0.4, point source,
@@ -616,7 +665,7 @@ def run_configs(args):
             "reference_cpu_s_per_solve": ref_s, "cpu_threads": threads,
             "fp64_column0_rel_err_vs_reference": err_ref,
             "speedup_vs_reference_cpu": None if ref_s is None else ref_s / (ms_m / 12 * 1e-3)}
-    print(json.dumps({"workload": "configurations below the headline volume", "results": res}), flush=True)
+    return {"workload": "configurations below the headline volume", "results": res}
 
 
 CLOVER_WORKLOAD = dict(name="twisted-clover e/o CG solve (inv_tmclovD_cg_eoprec), 32^3x64, cSW 1.6, point sources, "
@@ -671,10 +720,10 @@ SERVE_WORKLOAD = dict(volumes={"8^3x16": (16, 8), "16^3x32": (32, 16), "32^3x64"
                       probs=[0.5, 0.35, 0.15], eps=0.35, seed=1, rate=20.0, requests=200, nslots=16)
 
 
-def run_serve(args):
+def leg_serve(args):
     """The serving workload: three resident configurations, Poisson arrivals
-    at a stated rate, requests batched continuously per volume; prints p50/p99
-    latency and throughput (an extra report, not the headline)."""
+    at a stated rate, requests batched continuously per volume; p50/p99
+    latency and throughput."""
     from nissa_b200 import workload as wl
     from nissa_b200.serve import GpuResidency, SolveServer, latency_summary, poisson_requests, run_load
     W = SERVE_WORKLOAD
@@ -695,7 +744,7 @@ def run_serve(args):
                  "max_true_rel_res2_over_target": max(r.stats["true_rel_res2"] / r.request.residue for r in results),
                  "failed": sum(r.stats["status"] != 0 for r in results), "clocks": clk.summary()})
     res.close()
-    print(json.dumps(summ), flush=True)
+    return summ
 
 
 def main():
@@ -705,8 +754,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--fp64-iters", type=int, default=FP64_ITERS,
-                    help="FP64 CG iterations of one full solve (scales the reference arm's bounded sample)")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the other configurations (16^3x32 and 8^3x16 columns, 48-RHS batched, multi-shift, "
+                         "serving) that the headline line carries as sub-objects")
     ap.add_argument("--lattice", default=None, help="T,L override for quick checks (not the benchmark workload)")
     ap.add_argument("--kernel-only", default=None, choices=["double", "single", "half"],
                     help="only time the e/o hopping kernel of this precision (profiling entry point)")
@@ -714,7 +764,8 @@ def main():
     ap.add_argument("--nrep", type=int, default=10, help="launches for --kernel-only")
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
-    ap.add_argument("--hop-cfg", type=int, default=-1, help="hopping-kernel launch shape for --kernel-only (tuning)")
+    ap.add_argument("--hop-cfg", type=int, default=-1,
+                    help="hopping-kernel launch shape of the inner precision (tuning; default: the library's)")
     ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve", "batched", "configs", "clover"],
                     help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop; "
                          "batched: 48 right-hand sides batched vs one at a time; configs: the 8^3x16 and "
@@ -734,17 +785,9 @@ def main():
     if args.kernel_only:
         run_kernel_only(args)
         return
-    if args.workload == "cgm":
-        run_cgm(args)
-        return
-    if args.workload == "serve":
-        run_serve(args)
-        return
-    if args.workload == "batched":
-        run_batched(args)
-        return
-    if args.workload == "configs":
-        run_configs(args)
+    legs = {"cgm": leg_cgm, "serve": leg_serve, "batched": leg_batched, "configs": leg_configs}
+    if args.workload in legs:
+        print(json.dumps(legs[args.workload](args)), flush=True)
         return
     if args.workload == "clover":
         run_clover(args)
@@ -753,12 +796,6 @@ def main():
         run_reference_arm(args)
     else:
         run_ours(args)
-
-
-# FP64 CG iterations of one full solve of this workload (measured on the GPU's
-# plain FP64 CG, which matches the reference's iteration count; printed by each
-# run of this script under "fp64.iterations").
-FP64_ITERS = 99
 
 if __name__ == "__main__":
     main()
