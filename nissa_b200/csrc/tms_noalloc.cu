@@ -11,10 +11,19 @@
 //
 // The array is a file-scope __device__ variable of TMS_NOALLOC_MAX_SITES * 768
 // + 256 bytes (12 MiB): every GPU that loads this library holds it until the
-// process exits.  Every call shares it and it keeps the last call's contents;
-// calls whose work overlaps on the GPU (two streams, two host threads) race on
-// it and must be serialised by the caller.  Each call writes every scratch
-// element before reading it, so nothing has to start at zero.
+// process exits.  With CUDA's lazy module loading (the default) the library's
+// device code, and with it this array, is loaded onto a device the first time
+// it is needed there; the first call of tms_hop_eo_noalloc on a device does
+// that (its cudaGetSymbolAddress set-up forces the load), so that call is the
+// one that makes the 12 MiB appear and may synchronise: make it outside any
+// phase that must not see either.  Every call shares the array and it keeps
+// the last call's contents; calls whose work overlaps on the GPU (two streams,
+// two host threads) race on it and must be serialised by the caller.  Each
+// call writes every scratch element before reading it, so nothing has to
+// start at zero.  The device address found at set-up is kept per device
+// ordinal for the life of the process; after cudaDeviceReset the module is
+// reloaded and may sit elsewhere, so this entry point is not for use across a
+// device reset.
 #include "tmsolve.h"
 #include "tms_kernels.cuh"
 

@@ -34,25 +34,36 @@ def _noalloc(lib, T, L, conf_dev, par_out, in_dev, out_dev, anis=None, layout=0,
     return st, err.value.decode()
 
 
-def test_noalloc_hop_matches_context_hop(cuda_device):
+@pytest.mark.parametrize("layout,bc_included", [("lx", False), ("eo", False), ("lx", True), ("eo", True)])
+def test_noalloc_hop_matches_context_hop(cuda_device, layout, bc_included):
+    """Both conf layouts (lx and e/o rows) and both boundary forms (periodic
+    links, or the time sign already folded into the t=T-1 links), each passed
+    identically to the ordinary entry point and to the allocation-free one."""
     import torch
+    import oracle
     lib = _lib.load()
     T, L = 16, 8  # 8192 sites: within TMS_NOALLOC_MAX_SITES
     conf = wl.gauge_conf(T, L, 0.4, seed=31)
+    if bc_included:
+        conf = wl.apply_time_bc(conf, T, L, -1.0)
+    if layout == "eo":
+        conf = oracle.Geom(T, L).split(conf)
     Vh = T * L ** 3 // 2
     x0 = wl.random_spinor(Vh, 32)
     x1 = wl.random_spinor(Vh, 33)
     with Lattice(T, L, bc_t=-1.0) as lat:
-        lat.upload_conf(conf)
+        lat.upload_conf(conf, layout=layout, bc_included=bc_included)
         ref0 = lat.tmn2Deo_or_tmn2Doe_eos(0, x0)
         ref1 = lat.tmn2Deo_or_tmn2Doe_eos(1, x1, anis=1.2)
-    conf_d = torch.from_numpy(conf).cuda()
+    conf_d = torch.from_numpy(np.ascontiguousarray(conf)).cuda()
     out_d = torch.empty((Vh, 4, 3, 2), dtype=torch.float64, device="cuda")
-    # first call (sets the scratch up on this device), then a second call that reuses it
-    st, msg = _noalloc(lib, T, L, conf_d, 0, torch.from_numpy(x0).cuda(), out_d)
+    lay = 0 if layout == "lx" else 1
+    flags = 1 if bc_included else 0  # TMS_CONF_BC_INCLUDED
+    # two calls in a row: the second reuses (and overwrites) the scratch the first one left
+    st, msg = _noalloc(lib, T, L, conf_d, 0, torch.from_numpy(x0).cuda(), out_d, layout=lay, flags=flags)
     assert st == 0, msg
     assert rel(out_d.cpu().numpy(), ref0) < TOL
-    st, msg = _noalloc(lib, T, L, conf_d, 1, torch.from_numpy(x1).cuda(), out_d, anis=1.2)
+    st, msg = _noalloc(lib, T, L, conf_d, 1, torch.from_numpy(x1).cuda(), out_d, anis=1.2, layout=lay, flags=flags)
     assert st == 0, msg
     assert rel(out_d.cpu().numpy(), ref1) < TOL
 
