@@ -61,8 +61,23 @@ HOP_KERNEL = {"half": "hopping kernel of the FP16 inner solver (16-bit 12-real l
                       "the first half of K (the library's launch shape for FP16 spinors)",
               "single": "hopping kernel of the FP32 inner solver (16-bit 12-real links) + inverse diagonal, "
                         "the first half of K (the library's launch shape for FP32 spinors)"}
-# DRAM bytes of one launch of that kernel on this workload, from ncu
-HOP_TRAFFIC = {"half": 298.2e6}
+# DRAM bytes of one launch of that kernel on this workload: read from the ncu
+# summary of the current kernel under profiles/ (its "dram bytes per launch" line)
+HOP_PROFILE = {"half": "hop_kernel_fp16_pipelined_32c64.md"}
+
+
+def hop_traffic(prec):
+    """(bytes, source) of the ncu capture of the inner hop, or (None, why)."""
+    import re
+    name = HOP_PROFILE.get(prec)
+    if not name:
+        return None, "no ncu capture of this kernel"
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            m = re.search(r"dram bytes per launch:\s*([0-9.e+]+)", f.read())
+        return (float(m.group(1)), "profiles/" + name) if m else (None, "profiles/%s has no traffic line" % name)
+    except OSError:
+        return None, "profiles/%s absent" % name
 
 
 def log(*a):
@@ -258,6 +273,16 @@ def run_ours(args):
     value = replicas.whole_job_rate(args.steps, ms_max, ws)
     clocks = clk.summary()
 
+    # --- roofline: the inner solver's hopping kernel, and the FP64 Dslash, timed right after ----
+    # --- the timed region (same clocks and power state) --------------------------------------
+    peak, peak_kind = peaks()
+    hop_prec = prec if prec != "double" else "single"
+    hop_ms, hop_bytes = lat.bench_hop(hop_prec, variant=1, nrep=30, flush=True)
+    d64_ms, d64_bytes = lat.bench_hop("double", variant=0, nrep=30, flush=True)
+    achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
+    d64_gbs = d64_bytes / (d64_ms * 1e-3) / 1e9
+    traffic, traffic_src = hop_traffic(hop_prec)
+
     # --- e2e: the same columns through the C ABI from pinned host buffers -------------------
     # (tms_cg_eoprec_columns: every column's source is copied in and its solution out inside
     # the timed region, the copies of the neighbouring columns overlapping each solve)
@@ -277,14 +302,6 @@ def run_ours(args):
     e2e_value = replicas.whole_job_rate(e2e_steps, replicas.max_over_ranks((time.perf_counter() - h0) * 1e3), ws)
     assert max(x["lx_rel_res2"] for x in e2e_stats) < 10 * residue
     bytes_per = V * 24 * 8
-
-    # --- roofline: the inner solver's hopping kernel, and the FP64 Dslash -------------------
-    peak, peak_kind = peaks()
-    hop_prec = prec if prec != "double" else "single"
-    hop_ms, hop_bytes = lat.bench_hop(hop_prec, variant=1, nrep=30, flush=True)
-    d64_ms, d64_bytes = lat.bench_hop("double", variant=0, nrep=30, flush=True)
-    achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
-    d64_gbs = d64_bytes / (d64_ms * 1e-3) / 1e9
 
     # --- plain FP64 GPU CG on the same solves, and the accuracy of the mixed solutions -------
     fp64_steps = 2
@@ -400,9 +417,9 @@ def run_ours(args):
                 "steps": e2e_steps},
         "roofline": {"bound": "hbm", "kernel": HOP_KERNEL[hop_prec],
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": HOP_TRAFFIC.get(hop_prec),
+                     "peak_kind": peak_kind, "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
-                                       "kernel on this workload (profiles/)",
+                                       "kernel on this workload (%s)" % traffic_src,
                      "ms_per_launch": hop_ms, "alg_bytes_per_launch": hop_bytes},
         "variants": variants,
         "batched_12_columns": batched,

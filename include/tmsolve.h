@@ -180,6 +180,37 @@ tms_status tms_cg_eoprec_batched(tms_ctx *ctx, int nrhs, double *const *sols_lx,
                                  double kappa, int has_anis, double anis, const double *mus, int niter,
                                  const double *residues, int precision, tms_stats *stats);
 
+/* ---- time-slab decomposition (replaces, for a split along time, the reference's halo exchange
+ * before each hop, base/field.cpp:11-56, and its all-reduce after each scalar product,
+ * base/field.hpp:904) ----
+ * A slab context owns the time slices [t0, t0 + T_loc) of a T x LX x LY x LZ lattice (t0, T_loc
+ * even); its conf is uploaded as the slab's own links in lx layout (tms_conf_upload: sites of the
+ * slab only, local t = 0 .. T_loc-1).  The time hops that leave the slab read two faces of
+ * tms_slab_face_sites(ctx) sites x 6 complex (double[face][6][2] laid out as six planes of face
+ * complex: plane k = colour k of h0 (k < 3) or colour k-3 of h1) that the neighbouring slabs pack:
+ *   face_fwd: packed by the NEXT slab from its first slice (the forward (1 - g_t) projection),
+ *   face_bwd: packed by the PREVIOUS slab from its last slice (U_t^+ times the backward projection),
+ * so no link crosses a slab boundary.  The time-boundary sign is applied by the slab that receives
+ * across t = T-1 -> 0 (the bc_t given at creation).  Slab operators are exactly the single-context
+ * ones on the whole lattice. */
+tms_status tms_create_slab(tms_ctx **ctx, int T, int t0, int T_loc, int LX, int LY, int LZ, double bc_t, int device);
+/* sites of one parity on one time slice (LX LY LZ / 2): the length of a face */
+int64_t tms_slab_face_sites(const tms_ctx *ctx);
+/* Pack the two faces of e/o spinor `in` (parity par_in, Vh x 24 AoS): face_fwd for the previous
+ * slab, face_bwd for the next one (each face_sites x 12 doubles). */
+tms_status tms_slab_pack(tms_ctx *ctx, int par_in, const double *in, double *face_fwd, double *face_bwd);
+/* tmn2Deo_or_tmn2Doe_eos on the slab: out (parity par_out) from in (the other parity) and the two
+ * faces received for `in` (ghost_fwd from the next slab, ghost_bwd from the previous one). */
+tms_status tms_slab_hop(tms_ctx *ctx, int par_out, const double *in, const double *ghost_fwd, const double *ghost_bwd,
+                        double *out, int has_anis, double anis);
+/* The two halves of tmDkern_eoprec_eos (dirac_operator_tmD_eoprec_portable.cpp:36-51) on the slab:
+ * which = 0: out_even = (1/2k + i mu g5)^-1 D_eo in_odd; which = 1: out_odd = g5 ((1/2k + i mu g5) x
+ * - D_oe in_even / 4), x the odd operand of the first half.  Faces as for tms_slab_hop, packed from
+ * the half's own input. */
+tms_status tms_slab_kern_half(tms_ctx *ctx, int which, double kappa, double mu, const double *in,
+                              const double *ghost_fwd, const double *ghost_bwd, const double *x, double *out,
+                              int has_anis, double anis);
+
 /* ---- batch sessions (continuous batching; no reference counterpart) ----
  * A session keeps up to nslots (<= 64) solves of inv_tmD_cg_eoprec in flight on one context, each
  * with its own kappa, mu and residue: submit puts a right-hand side into a free slot (the source is
@@ -297,8 +328,12 @@ int64_t tms_hop_stage_timeouts(tms_ctx *ctx);
  * 12-real links, 1 (default): 16-bit fixed-point 12-real links, as fast or faster from 8^3x16 to 32^3x64), "links_reliable" (1 (default): the FP64
  * residual recomputations of the mixed solvers read the links as 12 reals, row 2 rebuilt, when the conf
  * is SU(3) to 1e-13; 0: always 18 reals), "mrhs_per_thread" (right-hand sides one thread of the
- * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2),
+ * batched hopping kernel computes from each link it loads: 1, 2, 4; FP64 uses at most 2; 0: one, with
+ * its gathers streamed through the thread's shared-memory slots by cp.async, FP32 arithmetic only),
  * "batch_graph_iters" (CG iterations per batch-session graph block, 0: chosen by batch size),
+ * "cgm_refine_batched" (mixed multi-shift solver: 0 (default) corrects the shifts one after the other
+ * through the e/o solver, 1 corrects all shifts as two batched e/o solves per round, one right-hand
+ * side per shift), 
  * "stream_priority" (the context's stream is recreated with this CUDA stream priority, an integer in the
  * device's range, lower first; contexts of small volumes sharing a GPU with large ones use it).  Results do not depend on the launch shapes. */
 tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);

@@ -50,6 +50,11 @@ SIGNATURES = {
     "tms_conf_load_ildg": (I, [P, ctypes.c_char_p, I]),
     "tms_conf_plaquette": (I, [P, I, ctypes.POINTER(D)]),
     "tms_hop_eo": (I, [P, I, P, P, I, D]),
+    "tms_create_slab": (I, [ctypes.POINTER(P), I, I, I, I, I, I, D, I]),
+    "tms_slab_face_sites": (ctypes.c_int64, [P]),
+    "tms_slab_pack": (I, [P, I, P, P, P]),
+    "tms_slab_hop": (I, [P, I, P, P, P, P, I, D]),
+    "tms_slab_kern_half": (I, [P, I, D, D, P, P, P, P, P, I, D]),
     "tms_tmDee": (I, [P, D, D, P, P]),
     "tms_inv_tmDee": (I, [P, D, D, P, P]),
     "tms_kern_eoprec": (I, [P, D, I, D, D, P, P]),

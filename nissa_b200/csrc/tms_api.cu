@@ -178,6 +178,7 @@ tms_status tms_destroy(tms_ctx* ctx)
   fr(ctx->red_partial);
   fr(ctx->red_counter);
   fr(ctx->tma_timeouts);
+  fr(ctx->slab_ghost);
   fr(ctx->red_result);
   fr(ctx->stage);
   for (double*& b : ctx->colbuf) fr(b);
@@ -444,6 +445,12 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       ctx->graph_iters = v;
       return TMS_OK;
     }
+  if (k == "cgm_refine_batched")
+    {
+      if (value != 0.0 && value != 1.0) return fail(ctx, TMS_ERR_BAD_ARG, "cgm_refine_batched: 0 or 1");
+      ctx->cgm_refine_batched = (int)value;
+      return TMS_OK;
+    }
   if (k == "cgm_floor_single")
     {
       if (!(value >= 1e-20 && value < 1.0)) return fail(ctx, TMS_ERR_BAD_ARG, "cgm_floor_single: in [1e-20, 1)");
@@ -483,7 +490,8 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
   if (k == "mrhs_per_thread")
     {
       const int v = (int)value;
-      if (v != 1 && v != 2 && v != 4) return fail(ctx, TMS_ERR_BAD_ARG, "mrhs_per_thread: 1, 2 or 4");
+      if (v != 0 && v != 1 && v != 2 && v != 4 || v != value)
+        return fail(ctx, TMS_ERR_BAD_ARG, "mrhs_per_thread: 0 (1, pipelined), 1, 2 or 4");
       if (ctx->mrhs_r != v && ctx->bw && ctx->bw_free)
         {
           cudaStreamSynchronize(ctx->stream);

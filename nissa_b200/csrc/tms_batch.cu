@@ -153,6 +153,18 @@ namespace
     if (P == PREC_F64 && r > 2) r = 2; // FP64 accumulators: 48 registers per right-hand side
     while (r > 1 && r > nrhs) r >>= 1;
     const int threads = MRHS_WARPS * 32;
+    if constexpr (P != PREC_F64)
+      if (r == 0)
+        {
+          // one right-hand side per thread, gathers pipelined through shared memory
+          constexpr int smem = SppFmt<P, LF>::template smem<MrhsPipe<P>::DIST>();
+          auto k = hop_mrhs_kernel<P, LF, Epi, Fin, 1, true>;
+          static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          (void)attr;
+          k<<<w->grid, threads, smem, s>>>(c->g, par_out, nrhs, bview<P>(in), U, w->bp, epi, w->red, fin, st);
+          return;
+        }
+    if (r < 1) r = 1;
 #define TMS_MRHS(RR)                                                                                             \
   hop_mrhs_kernel<P, LF, Epi, Fin, RR><<<w->grid, threads, 0, s>>>(c->g, par_out, nrhs, bview<P>(in), U, w->bp, epi, \
                                                                    w->red, fin, st)

@@ -13,6 +13,7 @@
 #pragma once
 
 #include "tms_kernels.cuh"
+#include "tms_hop_sp.cuh"
 
 namespace tms
 {
@@ -214,7 +215,7 @@ namespace tms
   // One parity (par_out) for nrhs right-hand sides, register-blocked: a
   // thread computes one site for R right-hand sides at once, so each link is
   // loaded (and rebuilt) once into registers and applied to the R neighbour
-  // spinors.  A warp takes 32 consecutive sites and the groups of R
+  // spinors (in FP32 arithmetic with the spin rows in packed lanes).  A warp takes 32 consecutive sites and the groups of R
   // right-hand sides one after the other (the links of its sites stay in L1
   // across groups).
   // A right-hand side whose state says stop is skipped.  Per right-hand side
@@ -249,20 +250,66 @@ namespace tms
         }
   }
 
+  // The FP32-arithmetic form (FP32 and FP16 spinors): the link of a direction
+  // is loaded and rebuilt once, then applied to the R right-hand sides with the
+  // two spin rows of each half spinor in the lanes of packed FP32 instructions
+  // (sp_dir_compute); 16-bit links keep row 2 in raw^2 units, scaled on the
+  // packed pairs.
+  template <int MU, bool FWD, int P, int LF, int R>
+  __device__ __forceinline__ void hop_dir_multi_sp(const Lattice& g, const Site& s, int p, int ieo,
+                                                   const SpinorBatch<P>& in, int rhs0, unsigned on,
+                                                   const LinkT<LF>& U, float anis, C<P2> A01[R][3], C<P2> A23[R][3])
+  {
+    constexpr bool K2 = (LF == LINK_I16_12);
+    const float fmu = (MU > 0) ? anis : 1.0f;
+    bool w;
+    const int n = FWD ? nbr_up<MU>(g, s, w) : nbr_dw<MU>(g, s, w);
+    C<float> L[9];
+    float ls;
+    if constexpr (K2)
+      {
+        U.template load_rows<false>(FWD ? p : 1 - p, MU, FWD ? ieo : n, L);
+        row2_unscaled(L);
+        ls = LinkT<LF>::kUnit;
+      }
+    else
+      U.template load_scaled<false>(FWD ? p : 1 - p, MU, FWD ? ieo : n, L, ls);
+    const float f = (w ? fmu * float(g.bc_t) : fmu) * ls;
+#pragma unroll
+    for (int j = 0; j < R; j++)
+      if (on & (1u << j))
+        {
+          C<float> sp[12];
+          float ss;
+          in.rhs(rhs0 + j).load_raw(n, sp, ss);
+          sp_dir_compute<MU, FWD, K2>(sp, L, f * ss, A01[j], A23[j], LinkT<LF>::kUnit);
+        }
+  }
+
   // resident blocks the register budget is capped for: more right-hand sides
   // per thread need more accumulator registers
   template <int P, int R>
   struct MrhsMinBlocks
   {
-    static constexpr int value = (P == PREC_F64) ? (R == 1 ? 3 : 2) : (R == 1 ? 6 : R == 2 ? 4 : 2);
+    static constexpr int value = (P == PREC_F64) ? (R == 1 ? 3 : 2) : (R == 1 ? 5 : R == 2 ? 4 : 2);
   };
 
-  template <int P, int LF, class Epi, class Fin, int R>
-  __global__ void __launch_bounds__(MRHS_WARPS * 32, MrhsMinBlocks<P, R>::value)
+  // PIPE (FP32 arithmetic, R = 1): each right-hand side's gathers streamed
+  // through the thread's shared-memory slots by cp.async, DIST directions ahead
+  // (spp_hop_site); the block's dynamic shared memory is SppFmt::smem<DIST>()
+  template <int P>
+  struct MrhsPipe
+  {
+    static constexpr int DIST = (P == PREC_F16) ? 3 : 2;
+  };
+
+  template <int P, int LF, class Epi, class Fin, int R, bool PIPE = false>
+  __global__ void __launch_bounds__(MRHS_WARPS * 32, PIPE ? (P == PREC_F16 ? 5 : 3) : MrhsMinBlocks<P, R>::value)
     hop_mrhs_kernel(Lattice g, int par_out, int nrhs, SpinorBatch<P> in, LinkT<LF> U, const BatchParams* __restrict__ bp,
                     Epi epi, BatchReducer red, Fin fin, const CgState* __restrict__ st)
   {
     using Re = typename SpinorT<P>::R;
+    extern __shared__ __align__(16) char mrhs_smem[];
     __shared__ double sh[Epi::kReduce ? MRHS_WARPS * MRHS_MAX : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int ngroups = (nrhs + R - 1) / R;
@@ -290,23 +337,68 @@ namespace tms
             for (int j = 0; j < R; j++) part[j] = 0.0;
             if (ieo < g.Vh)
               {
-                C<Re> acc[R][12];
-#pragma unroll
-                for (int j = 0; j < R; j++)
-#pragma unroll
-                  for (int k = 0; k < 12; k++) acc[j][k] = {Re(0), Re(0)};
                 const Site s = eo_site(g, par_out, ieo);
-                hop_dir_multi<0, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
-                hop_dir_multi<0, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
-                hop_dir_multi<1, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
-                hop_dir_multi<1, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
-                hop_dir_multi<2, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
-                hop_dir_multi<2, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
-                hop_dir_multi<3, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
-                hop_dir_multi<3, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                if constexpr (PIPE && P != PREC_F64 && R == 1)
+                  {
+                    C<float> acc[12];
+                    spp_hop_site<P, LF, MrhsPipe<P>::DIST>(mrhs_smem, g, par_out, ieo, in.rhs(rhs0), U, float(anis),
+                                                           acc);
+                    part[0] = epi(rhs0, ieo, *bp, acc);
+                  }
+                else if constexpr (P == PREC_F64)
+                  {
+                    C<Re> acc[R][12];
 #pragma unroll
-                for (int j = 0; j < R; j++)
-                  if (on & (1u << j)) part[j] = epi(rhs0 + j, ieo, *bp, acc[j]);
+                    for (int j = 0; j < R; j++)
+#pragma unroll
+                      for (int k = 0; k < 12; k++) acc[j][k] = {Re(0), Re(0)};
+                    hop_dir_multi<0, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                    hop_dir_multi<0, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                    hop_dir_multi<1, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                    hop_dir_multi<1, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                    hop_dir_multi<2, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                    hop_dir_multi<2, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                    hop_dir_multi<3, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+                    hop_dir_multi<3, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, acc);
+#pragma unroll
+                    for (int j = 0; j < R; j++)
+                      if (on & (1u << j)) part[j] = epi(rhs0 + j, ieo, *bp, acc[j]);
+                  }
+                else
+                  {
+                    C<P2> A01[R][3], A23[R][3];
+#pragma unroll
+                    for (int j = 0; j < R; j++)
+#pragma unroll
+                      for (int c = 0; c < 3; c++)
+                        {
+                          A01[j][c] = {p2(0.f, 0.f), p2(0.f, 0.f)};
+                          A23[j][c] = {p2(0.f, 0.f), p2(0.f, 0.f)};
+                        }
+                    hop_dir_multi_sp<0, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+                    hop_dir_multi_sp<0, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+                    hop_dir_multi_sp<1, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+                    hop_dir_multi_sp<1, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+                    hop_dir_multi_sp<2, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+                    hop_dir_multi_sp<2, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+                    hop_dir_multi_sp<3, true, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+                    hop_dir_multi_sp<3, false, P, LF, R>(g, s, par_out, ieo, in, rhs0, on, U, anis, A01, A23);
+#pragma unroll
+                    for (int j = 0; j < R; j++)
+                      if (on & (1u << j))
+                        {
+                          C<float> acc[12];
+#pragma unroll
+                          for (int c = 0; c < 3; c++)
+                            {
+                              acc[c] = {A01[j][c].re.v.x, A01[j][c].im.v.x};
+                              acc[3 + c] = {A01[j][c].re.v.y, A01[j][c].im.v.y};
+                              acc[6 + c] = {A23[j][c].re.v.x, A23[j][c].im.v.x};
+                              acc[9 + c] = {A23[j][c].re.v.y, A23[j][c].im.v.y};
+                            }
+                          part[j] = epi(rhs0 + j, ieo, *bp, acc);
+                        }
+                  }
               }
             if (Epi::kReduce)
 #pragma unroll

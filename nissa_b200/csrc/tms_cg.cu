@@ -841,6 +841,153 @@ namespace
   }
 }
 
+namespace
+{
+  // the reference's chiral gamma5 on lx AoS spinors (spins 2, 3 negated), in place
+  __global__ void aos_g5_kernel(int64_t nsites, double* __restrict__ a)
+  {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsites * 12) return;
+    const int64_t site = i / 12, k = i % 12;
+    a[site * 24 + 12 + k] = -a[site * 24 + 12 + k];
+  }
+
+  // y += x over n doubles
+  __global__ void aos_axpy_kernel(int64_t n, const double* __restrict__ x, double* __restrict__ y)
+  {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += x[i];
+  }
+
+  struct DevArrays
+  {
+    std::vector<double*> p;
+    ~DevArrays()
+    {
+      for (double* q : p)
+        if (q) cudaFree(q);
+    }
+  };
+
+  // Mixed multi-shift: every shift's FP32 multi-shift solution brought to its
+  // target by defect correction through the e/o solver, all shifts at once:
+  // (Q_W^2 + m^2)^-1 = Q(-m)^-1 Q(+m)^-1 and Q(mu)^-1 = D(mu)^-1 g5, so one
+  // round is e_k = D(-m_k)^-1 g5 D(+m_k)^-1 g5 r_k for all unconverged shifts
+  // as two batched e/o solves (one right-hand side per shift, per-shift mu),
+  // then x_k += e_k and the FP64 true residual r_k = b - (Q_W^2 + m_k^2) x_k.
+  // Each e/o solve goes to a tenth of the shift's remaining squared factor.
+  tms_status cgm_refine_batched(tms_ctx* ctx, double kappa, int has_anis, double anis, const double* masses, int nmass,
+                                int niter, const double* residues, int precision, double b2, tms_status st0,
+                                int iters, float ms, double* const* sols, tms_stats* stats)
+  {
+    Field* f = ctx->lx64;
+    const int64_t V = ctx->g.V;
+    const size_t bytes = (size_t)V * 24 * sizeof(double);
+    DevArrays X, Rg, Y, E;
+    for (DevArrays* a : {&X, &Rg, &Y, &E})
+      {
+        a->p.assign(nmass, nullptr);
+        for (int k = 0; k < nmass; k++) CU(cudaMalloc(&a->p[k], bytes));
+      }
+    const int saved_mode = ctx->ptr_mode;
+    struct ModeGuard
+    {
+      tms_ctx* c;
+      int m;
+      ~ModeGuard() { c->ptr_mode = m; }
+    } guard{ctx, saved_mode};
+    ctx->ptr_mode = TMS_PTR_DEVICE;
+    const int blk = 256;
+    const unsigned g5grid = (unsigned)div_up(V * 12, (int64_t)blk), axgrid = (unsigned)div_up(V * 24, (int64_t)blk);
+    std::vector<double> rt(nmass);
+    std::vector<tms_stats> sk(nmass);
+    // the multi-shift solutions, their true residues and g5 r
+    for (int k = 0; k < nmass; k++)
+      {
+        cgm_solution<PREC_F32>(ctx, k, f[1]);
+        TRY(set_params(ctx, kappa, masses[k], has_anis, anis));
+        TRY(LxOp::true_residual(ctx, f[0], f[1], f[2], &rt[k]));
+        fill_stats(&sk[k], st0, iters, 0, ctx->cgm_h->res[k], rt[k] / b2, ms);
+        TRY(lx_out(ctx, f[1], X.p[k]));
+        TRY(lx_out(ctx, f[2], Rg.p[k]));
+        ++ctx->launches;
+        aos_g5_kernel<<<g5grid, blk, 0, ctx->stream>>>(V, Rg.p[k]);
+      }
+    CU(cudaGetLastError());
+    tms_status worst = TMS_OK;
+    for (int round = 0; round < 4; round++)
+      {
+        std::vector<int> act;
+        for (int k = 0; k < nmass; k++)
+          if (rt[k] >= residues[k] * b2) act.push_back(k);
+        if (act.empty()) break;
+        const int na = (int)act.size();
+        std::vector<double*> src(na), sol(na);
+        std::vector<double> mu(na), rel(na);
+        std::vector<tms_stats> es(na);
+        for (int a = 0; a < na; a++)
+          {
+            const int k = act[a];
+            rel[a] = std::min(1e-2, std::max(1e-22, 1e-1 * residues[k] * b2 / rt[k]));
+          }
+        for (int pass = 0; pass < 2; pass++)
+          {
+            for (int a = 0; a < na; a++)
+              {
+                const int k = act[a];
+                src[a] = pass ? Y.p[k] : Rg.p[k];
+                sol[a] = pass ? E.p[k] : Y.p[k];
+                mu[a] = pass ? -masses[k] : masses[k];
+              }
+            const tms_status s = tms_cg_eoprec_batched(ctx, na, sol.data(), src.data(), kappa, has_anis, anis,
+                                                       mu.data(), niter, rel.data(), precision, es.data());
+            if (s != TMS_OK && s != TMS_ERR_NOT_CONVERGED) return s;
+            if (s != TMS_OK) worst = s;
+            for (int a = 0; a < na; a++)
+              {
+                sk[act[a]].iterations += es[a].iterations;
+                sk[act[a]].seconds += es[a].seconds;
+                ++ctx->launches;
+                if (pass == 0) aos_g5_kernel<<<g5grid, blk, 0, ctx->stream>>>(V, Y.p[act[a]]);
+                else aos_axpy_kernel<<<axgrid, blk, 0, ctx->stream>>>(V * 24, E.p[act[a]], X.p[act[a]]);
+              }
+            CU(cudaGetLastError());
+          }
+        for (int a = 0; a < na; a++)
+          {
+            const int k = act[a];
+            TRY(lx_in(ctx, X.p[k], f[1]));
+            TRY(set_params(ctx, kappa, masses[k], has_anis, anis));
+            TRY(LxOp::true_residual(ctx, f[0], f[1], f[2], &rt[k]));
+            TRY(lx_out(ctx, f[2], Rg.p[k]));
+            ++ctx->launches;
+            aos_g5_kernel<<<g5grid, blk, 0, ctx->stream>>>(V, Rg.p[k]);
+            sk[k].reliable_updates++;
+          }
+        CU(cudaGetLastError());
+      }
+    ctx->ptr_mode = saved_mode;
+    for (int k = 0; k < nmass; k++)
+      {
+        const tms_status sk_st = (rt[k] >= residues[k] * b2) ? TMS_ERR_NOT_CONVERGED : (worst == TMS_ERR_NOT_CONVERGED ? TMS_OK : worst);
+        sk[k].true_rel_res2 = rt[k] / b2;
+        sk[k].iterated_rel_res2 = rt[k] / b2;
+        sk[k].status = sk_st;
+        if (sk_st != TMS_OK) worst = TMS_ERR_NOT_CONVERGED;
+        if (stats) stats[k] = sk[k];
+        if (saved_mode == TMS_PTR_HOST)
+          {
+            CU(cudaMemcpyAsync(sols[k], X.p[k], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+          }
+        else
+          CU(cudaMemcpyAsync(sols[k], X.p[k], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+      }
+    CU(cudaStreamSynchronize(ctx->stream));
+    return worst;
+  }
+}
+
 extern "C" {
 
 tms_status tms_cg_eoprec(tms_ctx* ctx, double* sol_lx, const double* src_lx, double kappa, int has_anis, double anis,
@@ -1054,6 +1201,18 @@ tms_status tms_cgm_tmQ2(tms_ctx* ctx, double* const* sols, const double* src_lx,
     st = ctx->su3 ? cgm_run<PREC_F32>(ctx, links32r(ctx), nmass, sigma, target, niter, b2, &iters, &ms)
                   : cgm_run<PREC_F32>(ctx, links32f(ctx), nmass, sigma, target, niter, b2, &iters, &ms);
   if (st != TMS_OK && st != TMS_ERR_NOT_CONVERGED) return st;
+  if (precision != TMS_PREC_DOUBLE && ctx->cgm_refine_batched)
+    {
+      // all shifts' corrections as batched e/o solves (tuning "cgm_refine_batched")
+      tms_status worst = st;
+      const tms_status s2 = cgm_refine_batched(ctx, kappa, has_anis, anis, masses, nmass, niter, residues, precision,
+                                               b2, st, iters, ms, sols, stats);
+      if (s2 != TMS_OK && s2 != TMS_ERR_NOT_CONVERGED) return s2;
+      if (s2 != TMS_OK) worst = s2;
+      TRY(finish(ctx));
+      if (worst != TMS_OK) return fail(ctx, worst, "exit without converging");
+      return TMS_OK;
+    }
   tms_status worst = st;
   for (int k = 0; k < nmass; k++)
     {

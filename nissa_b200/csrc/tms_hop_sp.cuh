@@ -395,12 +395,60 @@ namespace tms
     sp_dir_compute<MU, (D % 2) == 0, LF == LINK_I16_12>(sp, L, f, A01, A23, 1.0f / 32767.0f);
   }
 
+  // the hop of site (p, ieo) with the thread's gathers pipelined through its
+  // slots of `smem` (SppFmt::smem<DIST>() bytes for the block), in the
+  // accumulator layout of hop_site
+  template <int P, int LF, int DIST>
+  __device__ __forceinline__ void spp_hop_site(char* smem, const Lattice& g, int p, int ieo, const SpinorT<P>& in,
+                                               const LinkT<LF>& U, float anis, C<float> acc[12])
+  {
+    constexpr int SLOTS = DIST + 1;
+    const SppSlots<P, LF, SLOTS> sl{smem, (int)(threadIdx.x % SPP_THREADS)};
+    const Site s = eo_site(g, p, ieo);
+    C<P2> A01[3], A23[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      {
+        A01[c] = {p2(0.f, 0.f), p2(0.f, 0.f)};
+        A23[c] = {p2(0.f, 0.f), p2(0.f, 0.f)};
+      }
+    bool w[8];
+    // the copies of the first DIST directions, one commit group each
+#define TMS_SPP_ISSUE(D)                                                                                           \
+  if ((D) < 8) spp_issue<((D) < 8 ? (D) : 0), P, LF, SLOTS>(sl, (D) % SLOTS, g, s, p, ieo, in, U, w[(D) < 8 ? (D) : 0]); \
+  cp_async_commit();
+#define TMS_SPP_STEP(D)                                                                                            \
+  TMS_SPP_ISSUE((D) + DIST)                                                                                        \
+  cp_async_wait<DIST>();                                                                                           \
+  spp_compute<D, P, LF, SLOTS>(sl, g, w[D], anis, A01, A23);
+    TMS_SPP_ISSUE(0)
+    if (DIST > 1) { TMS_SPP_ISSUE(1) }
+    if (DIST > 2) { TMS_SPP_ISSUE(2) }
+    TMS_SPP_STEP(0)
+    TMS_SPP_STEP(1)
+    TMS_SPP_STEP(2)
+    TMS_SPP_STEP(3)
+    TMS_SPP_STEP(4)
+    TMS_SPP_STEP(5)
+    TMS_SPP_STEP(6)
+    TMS_SPP_STEP(7)
+#undef TMS_SPP_STEP
+#undef TMS_SPP_ISSUE
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      {
+        acc[c] = {A01[c].re.v.x, A01[c].im.v.x};
+        acc[3 + c] = {A01[c].re.v.y, A01[c].im.v.y};
+        acc[6 + c] = {A23[c].re.v.x, A23[c].im.v.x};
+        acc[9 + c] = {A23[c].re.v.y, A23[c].im.v.y};
+      }
+  }
+
   template <int P, int LF, class Epi, class Fin, int DIST, int MINB = 1>
   __global__ void __launch_bounds__(SPP_THREADS, MINB)
     hop_spp_kernel(Lattice g, int par_out, int npar, SpinorT<P> in_e, SpinorT<P> in_o, LinkT<LF> U,
                    const OpParams* prm, Epi epi, Reducer red, Fin fin, const int* __restrict__ stop)
   {
-    constexpr int SLOTS = DIST + 1;
     extern __shared__ __align__(16) char spp_smem[];
     pdl_enter();
     if (stop && *stop) return;
@@ -415,48 +463,8 @@ namespace tms
     double part = 0.0;
     if (active)
       {
-        const SppSlots<P, LF, SLOTS> sl{spp_smem, (int)threadIdx.x};
-        const SpinorT<P> in = p ? in_e : in_o;
-        const Site s = eo_site(g, p, ieo);
-        const float anis = float(prm->anis);
-        C<P2> A01[3], A23[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-          {
-            A01[c] = {p2(0.f, 0.f), p2(0.f, 0.f)};
-            A23[c] = {p2(0.f, 0.f), p2(0.f, 0.f)};
-          }
-        bool w[8];
-        // the copies of the first DIST directions, one commit group each
-#define TMS_SPP_ISSUE(D)                                                                                           \
-  if ((D) < 8) spp_issue<((D) < 8 ? (D) : 0), P, LF, SLOTS>(sl, (D) % SLOTS, g, s, p, ieo, in, U, w[(D) < 8 ? (D) : 0]); \
-  cp_async_commit();
-#define TMS_SPP_STEP(D)                                                                                            \
-  TMS_SPP_ISSUE((D) + DIST)                                                                                        \
-  cp_async_wait<DIST>();                                                                                           \
-  spp_compute<D, P, LF, SLOTS>(sl, g, w[D], anis, A01, A23);
-        TMS_SPP_ISSUE(0)
-        if (DIST > 1) { TMS_SPP_ISSUE(1) }
-        if (DIST > 2) { TMS_SPP_ISSUE(2) }
-        TMS_SPP_STEP(0)
-        TMS_SPP_STEP(1)
-        TMS_SPP_STEP(2)
-        TMS_SPP_STEP(3)
-        TMS_SPP_STEP(4)
-        TMS_SPP_STEP(5)
-        TMS_SPP_STEP(6)
-        TMS_SPP_STEP(7)
-#undef TMS_SPP_STEP
-#undef TMS_SPP_ISSUE
         C<float> acc[12];
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-          {
-            acc[c] = {A01[c].re.v.x, A01[c].im.v.x};
-            acc[3 + c] = {A01[c].re.v.y, A01[c].im.v.y};
-            acc[6 + c] = {A23[c].re.v.x, A23[c].im.v.x};
-            acc[9 + c] = {A23[c].re.v.y, A23[c].im.v.y};
-          }
+        spp_hop_site<P, LF, DIST>(spp_smem, g, p, ieo, p ? in_e : in_o, U, float(prm->anis), acc);
         part = epi(p, ieo, acc);
       }
     if (Epi::kReduce) grid_reduce<SPP_THREADS>(part, red, fin);

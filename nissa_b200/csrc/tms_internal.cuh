@@ -72,6 +72,12 @@ struct tms_ctx
   unsigned* red_counter = nullptr;
   double* red_result = nullptr;
   unsigned* tma_timeouts = nullptr; // timed-out tile waits of the staged hop (launch shape 7); stays 0
+
+  // time-slab context (tms_create_slab): slices [slab_t0, slab_t0 + T) of a lattice of slab_T slices
+  bool slab = false;
+  int slab_T = 0, slab_t0 = 0;
+  double slab_bc_fwd = 1.0, slab_bc_bwd = 1.0; // signs of the faces crossing t = T-1 -> 0
+  void* slab_ghost = nullptr;                  // device copies of the two received faces
   double* red_h = nullptr;       // pinned
   int red_cap = 0;
   // Scalars cross between host and device through mapped page-locked memory
@@ -140,6 +146,7 @@ struct tms_ctx
   int mrhs_r = 1; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
   int pdl = 1;    // launch the CG iteration kernels with programmatic dependent launch
   double cgm_floor32 = 1e-12; // squared residue at which the FP32 multi-shift phase hands over to refinement
+  int cgm_refine_batched = 0; // mixed multi-shift: shifts corrected one after the other (0) or as batched solves (1)
 
   // batched-solver workspace (owned by tms_batch.cu)
   void* bw = nullptr;

@@ -8,7 +8,8 @@ solver) are the tuning knobs of the C ABI (tms_set_tuning):
                        gathers streamed through shared memory by cp.async,
                        row tiles staged by bulk copies)
   links_single         FP32 or 16-bit links under the FP32 inner solver
-  mrhs_per_thread      right-hand sides per thread of the batched kernel
+  mrhs_per_thread      right-hand sides per thread of the batched kernel (0:
+                       one, its gathers pipelined through shared memory)
 
 Each candidate is timed with the library's own kernel benchmarks (CUDA
 events, L2 flushed between launches), weighted as one CG iteration uses the
@@ -24,7 +25,7 @@ import os
 import threading
 
 HOP_SHAPES = {"double": (0, 1, 2), "single": (0, 1, 2, 3, 4, 5, 6, 7), "half": (0, 1, 2, 3, 4, 5, 6, 7)}
-MRHS_CHOICES = (1, 2, 4)
+MRHS_CHOICES = (0, 1, 2, 4)  # 0: one right-hand side per thread, gathers pipelined through shared memory
 
 _lock = threading.Lock()
 
@@ -88,7 +89,7 @@ def tune_batched(lat, precision: str, nrhs: int, nrep: int = 5) -> dict:
     """Pick the right-hand sides per thread of the batched kernel for nrhs."""
     best = None
     for r in MRHS_CHOICES:
-        if precision == "double" and r > 2:
+        if precision == "double" and (r > 2 or r == 0):
             continue
         lat.set_tuning("mrhs_per_thread", r)
         ms, _ = lat.bench_hop_batched(precision, nrhs=nrhs, nrep=nrep, flush=True)

@@ -322,15 +322,17 @@ def ref_available() -> bool:
 
 
 def run_ref(op: str, T: int, L: int, arrays: dict, out_shape, threads: int | None = None, out_dtype=np.float64,
-            **params):
-    """Run the reference's own code (oracle/_ref/nissa_ref) on raw arrays.
+            binary: str | None = None, env: dict | None = None, **params):
+    """Run the reference's own code (oracle/_ref/nissa_ref, or `binary`: the
+    same driver linked otherwise) on raw arrays.
 
     ``arrays`` maps 'conf'/'in' to numpy arrays; returns (output array or None,
     JSON record, stdout text)."""
-    if not ref_available():
-        raise RuntimeError("reference build missing: run oracle.build_ref()")
+    exe = binary or REF_BIN
+    if not os.path.exists(exe):
+        raise RuntimeError("%s missing: run oracle.build_ref()" % exe)
     with tempfile.TemporaryDirectory() as d:
-        argv = [REF_BIN, op, "T=%d" % T, "L=%d" % L]
+        argv = [exe, op, "T=%d" % T, "L=%d" % L]
         for k, a in arrays.items():
             path = os.path.join(d, k + ".bin")
             _c(a).tofile(path)
@@ -341,7 +343,7 @@ def run_ref(op: str, T: int, L: int, arrays: dict, out_shape, threads: int | Non
             if isinstance(v, (list, tuple, np.ndarray)):
                 v = ",".join(repr(float(x)) for x in v)
             argv.append("%s=%s" % (k, v))
-        env = dict(os.environ)
+        env = dict(os.environ, **(env or {}))
         env["NISSA_DO_NOT_TRAP_SIGNALS"] = "1"
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)

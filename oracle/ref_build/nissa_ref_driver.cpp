@@ -20,6 +20,7 @@
 //        hop conf in out par=P                   tmn2Deo_or_tmn2Doe_eos           (dirac_operator_tmD_eoprec_portable.hpp:33-169)
 //        kern conf in out kappa mu               tmDkern_eoprec_eos               (dirac_operator_tmD_eoprec_portable.cpp:36-51)
 //        kern2 conf in out kappa mu              tmDkern_eoprec_square_eos        (dirac_operator_tmD_eoprec_portable.cpp:54-65)
+//        kern2twice conf in out kappa mu         the same twice, the x links negated in place in between
 //        cg conf in out kappa mu niter residue   inv_tmDkern_eoprec_square_eos_cg (cg_invert_tmD_eoprec.cpp:61-78)
 //        cgfull conf in out kappa mu niter residue inv_tmD_cg_eoprec              (cg_invert_tmD_eoprec.cpp:152-213)
 //        tmQ conf in out kappa mu                apply_tmQ                        (dirac_operator_tmQ_portable.cpp:29-176)
@@ -447,6 +448,22 @@ int main(int narg, char** arg_v)
 		  const double t0 = now();
 		  for (int r = 0; r < reps; r++) tmDkern_eoprec_square_eos(out, temp1, temp2, conf, kappa, anis, mu, in);
 		  t_per_rep = (now() - t0) / reps;
+		}
+	      else if (op == "kern2twice")
+		{
+		  // K^2 twice on one EoField conf whose x links are negated in place in
+		  // between (the same allocations): a cache of the conf must notice
+		  OddField<spincolor> temp1("temp1", WITH_HALO), mid("mid", WITH_HALO);
+		  EvnField<spincolor> temp2("temp2", WITH_HALO);
+		  tmDkern_eoprec_square_eos(mid, temp1, temp2, conf, kappa, anis, mu, in);
+		  double* parts[2] = {conf.evenPart.template getPtr<MemorySpace::CPU>(),
+				      conf.oddPart.template getPtr<MemorySpace::CPU>()};
+		  for (double* c : parts)
+		    for (size_t i = 0; i < Vh; i++)
+		      for (int k = 18; k < 36; k++) c[i * 72 + k] = -c[i * 72 + k];
+		  conf.evenPart.invalidateHalo();
+		  conf.oddPart.invalidateHalo();
+		  tmDkern_eoprec_square_eos(out, temp1, temp2, conf, kappa, anis, mu, mid);
 		}
 	      else if (op == "cg" && args.count("sample_iters"))
 		{

@@ -12,8 +12,11 @@ from conftest import rel
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("precision", ["double", "single", "half"])
-def test_batched_matches_single_solves(cuda_device, precision):
+@pytest.mark.parametrize("precision,mrhs", [("double", 1), ("double", 2), ("single", 1), ("single", 0),
+                                            ("half", 0), ("half", 2), ("half", 4)])
+def test_batched_matches_single_solves(cuda_device, precision, mrhs):
+    """Every shape of the batched kernel: R right-hand sides per thread, or one
+    with its gathers pipelined through shared memory (mrhs 0)."""
     T, L = 16, 8
     kappa = 0.1610
     conf = wl.gauge_conf(T, L, 0.35, seed=51)
@@ -22,6 +25,7 @@ def test_batched_matches_single_solves(cuda_device, precision):
     res = [1e-20, 1e-20, 1e-18, 1e-20, 1e-16, 1e-20]
     with Lattice(T, L) as lat:
         lat.upload_conf(conf)
+        lat.set_tuning("mrhs_per_thread", mrhs)
         sols, st = lat.inv_tmD_cg_eoprec_batched(kappa, mus, srcs, 100000, res, precision=precision)
         for k in range(len(srcs)):
             ref, sref = lat.inv_tmD_cg_eoprec(kappa, mus[k], srcs[k], 100000, 1e-24, precision="double")

@@ -23,8 +23,10 @@ def test_cgm_double_matches_reference_fixture(cuda_device, golden_small):
             assert st[k]["true_rel_res2"] < 2e-20
 
 
-@pytest.mark.parametrize("precision", ["single", "half"])
-def test_cgm_mixed_reaches_every_target(cuda_device, precision):
+@pytest.mark.parametrize("precision,batched", [("single", 0), ("half", 0), ("half", 1)])
+def test_cgm_mixed_reaches_every_target(cuda_device, precision, batched):
+    """Both forms of the mixed solver's per-shift correction (shift after shift,
+    or all shifts as batched e/o solves) reach every target."""
     T, L = 16, 8
     kappa = 0.1632
     masses = np.array([0.005, 0.02, 0.08, 0.2])
@@ -34,6 +36,7 @@ def test_cgm_mixed_reaches_every_target(cuda_device, precision):
     ref, _, _ = geo.cgm(wl.apply_time_bc(conf, T, L), kappa, masses, np.full(4, 1e-24), src, 100000)
     with Lattice(T, L) as lat:
         lat.upload_conf(conf)
+        lat.set_tuning("cgm_refine_batched", batched)
         sols, st = lat.inv_tmQ2_cgm(kappa, masses, src, 100000, 1e-20, precision=precision)
         for k in range(len(masses)):
             assert st[k]["true_rel_res2"] < 1e-20, (k, st[k])
