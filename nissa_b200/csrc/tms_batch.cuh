@@ -250,11 +250,10 @@ namespace tms
         }
   }
 
-  // The FP32-arithmetic form (FP32 and FP16 spinors): the link of a direction
-  // is loaded and rebuilt once, then applied to the R right-hand sides with the
-  // two spin rows of each half spinor in the lanes of packed FP32 instructions
-  // (sp_dir_compute); 16-bit links keep row 2 in raw^2 units, scaled on the
-  // packed pairs.
+  // The FP16-spinor form: the link of a direction is loaded and rebuilt once,
+  // then applied to the R right-hand sides with the two spin rows of each half
+  // spinor in the lanes of packed FP32 instructions (sp_dir_compute); 16-bit
+  // links keep row 2 in raw^2 units, scaled on the packed pairs.
   template <int MU, bool FWD, int P, int LF, int R>
   __device__ __forceinline__ void hop_dir_multi_sp(const Lattice& g, const Site& s, int p, int ieo,
                                                    const SpinorBatch<P>& in, int rhs0, unsigned on,
@@ -345,8 +344,10 @@ namespace tms
                                                            acc);
                     part[0] = epi(rhs0, ieo, *bp, acc);
                   }
-                else if constexpr (P == PREC_F64)
+                else if constexpr (P != PREC_F16)
                   {
+                    // FP64, and FP32 spinors (whose float4 words do not pair the spin rows: the
+                    // packed form needs moves there and measured slower)
                     C<Re> acc[R][12];
 #pragma unroll
                     for (int j = 0; j < R; j++)

@@ -31,8 +31,6 @@ namespace tms
   // a - b, packed (no packed subtract: a fused multiply-add by -1)
   __device__ __forceinline__ P2 sub2(P2 a, P2 b) { return fma2(p2(-1.f, -1.f), b, a); }
 
-  // one direction from the neighbour's spinor sp (in stored units), its link L
-  // and the hop factor f that scales their product
   // row 2 of a special-unitary link from rows 0 and 1, conj(row0 x row1), in
   // the square of the rows' units (the caller scales its products)
   __device__ __forceinline__ void row2_unscaled(C<float> u[9])
@@ -42,6 +40,8 @@ namespace tms
     u[8] = cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));
   }
 
+  // One direction from the neighbour's spinor sp (in stored units), its link L
+  // and the hop factor f that scales their product.
   // With ROW2K, row 2 of L is in k2 times the units of rows 0 and 1 (16-bit
   // links: row 2 rebuilt from raw rows); its products are scaled by k2 on the
   // packed pairs (forward: the output row 2; backward: the input row h_2)
