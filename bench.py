@@ -63,15 +63,16 @@ HOP_KERNEL = {"half": "hopping kernel of the FP16 inner solver (16-bit 12-real l
                         "the first half of K (the library's launch shape for FP32 spinors)"}
 # DRAM bytes of one launch of that kernel on this workload: read from the ncu
 # summary of the current kernel under profiles/ (its "dram bytes per launch" line)
-HOP_PROFILE = {"half": "hop_kernel_fp16_pipelined_32c64.md"}
+# ncu captures of the inner hop on this workload, by (precision, launch shape)
+HOP_PROFILE = {("half", 6): "hop_kernel_fp16_pipelined_32c64.md"}
 
 
-def hop_traffic(prec):
+def hop_traffic(prec, shape):
     """(bytes, source) of the ncu capture of the inner hop, or (None, why)."""
     import re
-    name = HOP_PROFILE.get(prec)
+    name = HOP_PROFILE.get((prec, shape))
     if not name:
-        return None, "no ncu capture of this kernel"
+        return None, "no ncu capture of launch shape %d of this kernel" % shape
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
             m = re.search(r"dram bytes per launch:\s*([0-9.e+]+)", f.read())
@@ -227,8 +228,7 @@ def run_ours(args):
     lat = Lattice(T, L, bc_t=W["bc_t"], device=local)
     lat.upload_conf(conf)
     assert lat.conf_is_su3
-    if args.hop_cfg >= 0:
-        lat.set_tuning("hop_cfg_" + args.precision, args.hop_cfg)
+    tuning = headline_tuning(lat, args)
     plaquette = lat.plaquette()  # global_plaquette_lx_conf of the periodic links, on the device
 
     def column(k):
@@ -281,7 +281,7 @@ def run_ours(args):
     d64_ms, d64_bytes = lat.bench_hop("double", variant=0, nrep=30, flush=True)
     achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
     d64_gbs = d64_bytes / (d64_ms * 1e-3) / 1e9
-    traffic, traffic_src = hop_traffic(hop_prec)
+    traffic, traffic_src = hop_traffic(hop_prec, lat.get_tuning("hop_cfg_" + hop_prec))
 
     # --- e2e: the same columns through the C ABI from pinned host buffers -------------------
     # (tms_cg_eoprec_columns: every column's source is copied in and its solution out inside
@@ -421,6 +421,7 @@ def run_ours(args):
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
                                        "kernel on this workload (%s)" % traffic_src,
                      "ms_per_launch": hop_ms, "alg_bytes_per_launch": hop_bytes},
+        "tuning": tuning,
         "variants": variants,
         "batched_12_columns": batched,
         "fp64": {"solves_per_s": 1.0 / fp64_sec, "iterations": fp64_stats[0]["iterations"],
@@ -439,6 +440,51 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
+def headline_tuning(lat, args):
+    """The launch choices of the headline solve: the autotuner's (timed on this
+    lattice, cached per device and volume), or --hop-cfg / --tma-rows as given."""
+    prec = args.precision
+    if args.hop_cfg >= 0:
+        lat.set_tuning("hop_cfg_" + prec, args.hop_cfg)
+        if args.tma_rows >= 0:
+            lat.set_tuning("tma_rows", args.tma_rows)
+        return {"source": "command line", "settings": {"hop_cfg_" + prec: args.hop_cfg, "tma_rows": args.tma_rows}}
+    from nissa_b200 import tune
+    t0 = time.perf_counter()
+    r = tune.autotune(lat, prec)
+    out = {"source": "autotuner (cached)" if r["cached"] else "autotuner", "settings": r["settings"],
+           "ms_per_iteration": r["ms_per_iteration"], "alg_gbs": r["alg_gbs"],
+           "tuning_s": time.perf_counter() - t0,
+           "candidates": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in c.items()}
+                          for c in r["candidates"]]}
+    log("tuned: %s (%.1f s)" % (r["settings"], out["tuning_s"]))
+    return out
+
+
+TUNE_VOLUMES = [(16, 8), (32, 16), (48, 24), (64, 32)]
+
+
+def leg_tune(args):
+    """The autotuner's choice per volume (FP16 and FP32 inner hops, and the
+    12-RHS batched kernel): every candidate's device time and algorithmic
+    bandwidth, timed here into a fresh cache."""
+    import tempfile
+    from nissa_b200 import Lattice, tune
+    from nissa_b200 import workload as wl
+    out = {}
+    cache = os.path.join(tempfile.mkdtemp(), "tune.json")
+    for T, L in TUNE_VOLUMES:
+        conf = wl.gauge_conf(T, L, 0.35, 1, device="cuda:0")
+        with Lattice(T, L, bc_t=-1.0) as lat:
+            lat.upload_conf(conf)
+            name = "%d^3x%d" % (L, T)
+            out[name] = {p: tune.autotune(lat, p, cache=cache, retune=True) for p in ("half", "single")}
+            out[name]["half_batched_12"] = tune.autotune(lat, "half", nrhs=12, cache=cache, retune=True)
+        del conf
+        log("tuned %s" % name)
+    return {"workload": "autotuner per volume", "volumes": out}
+
+
 def run_kernel_only(args):
     """Profiling entry point: set up the workload's lattice and launch the e/o
     hopping kernel of one precision `nrep` times (L2 flushed between launches)."""
@@ -451,6 +497,8 @@ def run_kernel_only(args):
     lat.upload_conf(conf)
     if args.hop_cfg >= 0:
         lat.set_tuning("hop_cfg_" + args.kernel_only, args.hop_cfg)
+    if args.tma_rows >= 0:
+        lat.set_tuning("tma_rows", args.tma_rows)
     if args.nrhs > 1:
         if args.mrhs:
             lat.set_tuning("mrhs_per_thread", args.mrhs)
@@ -459,7 +507,8 @@ def run_kernel_only(args):
         ms, by = lat.bench_hop(args.kernel_only, variant=args.variant, nrep=args.nrep, flush=True)
     torch.cuda.synchronize()
     print(json.dumps({"kernel": "hop", "precision": args.kernel_only, "variant": args.variant, "nrhs": args.nrhs,
-                      "T": W["T"],
+                      "hop_cfg": lat.get_tuning("hop_cfg_" + args.kernel_only),
+                      "tma_rows": lat.get_tuning("tma_rows"), "T": W["T"],
                       "L": W["L"], "ms_per_launch": ms, "alg_bytes_per_launch": by,
                       "achieved_gbs": by / (ms * 1e-3) / 1e9}), flush=True)
 
@@ -747,7 +796,8 @@ def leg_serve(args):
     rate = args.rate or W["rate"]
     n = args.requests or W["requests"]
     vols = {k: (T, L, wl.gauge_conf(T, L, W["eps"], W["seed"], device="cuda:0")) for k, (T, L) in W["volumes"].items()}
-    res = GpuResidency(vols, nslots=W["nslots"], precision=args.serve_precision)
+    res = GpuResidency(vols, nslots=W["nslots"], precision=args.serve_precision,
+                       priorities=bool(args.serve_priorities))
     srv = SolveServer(res.backends(), free_memory=res.free_memory, reserve_bytes=2 << 30)
     warm = poisson_requests(6, rate=100.0, volumes=list(vols), probs=[1 / 3] * 3, seed=99)
     run_load(srv, warm)
@@ -758,6 +808,7 @@ def leg_serve(args):
     summ = latency_summary(results, wall)
     summ.update({"workload": "serving: resident 8^3x16, 16^3x32, 32^3x64; Poisson arrivals",
                  "rate_per_s": rate, "precision": args.serve_precision, "slots_per_volume": W["nslots"],
+                 "stream_priorities": "smaller volumes first" if args.serve_priorities else "equal",
                  "max_true_rel_res2_over_target": max(r.stats["true_rel_res2"] / r.request.residue for r in results),
                  "failed": sum(r.stats["status"] != 0 for r in results), "clocks": clk.summary()})
     res.close()
@@ -782,15 +833,20 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides for --kernel-only (batched kernel if > 1)")
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
     ap.add_argument("--hop-cfg", type=int, default=-1,
-                    help="hopping-kernel launch shape of the inner precision (tuning; default: the library's)")
-    ap.add_argument("--workload", default="cg", choices=["cg", "cgm", "serve", "batched", "configs", "clover"],
+                    help="hopping-kernel launch shape of the inner precision (default: the autotuner's)")
+    ap.add_argument("--tma-rows", type=int, default=-1,
+                    help="lattice rows per tile of the staged launch shape (with --hop-cfg or --kernel-only)")
+    ap.add_argument("--workload", default="cg",
+                    choices=["cg", "cgm", "serve", "batched", "configs", "clover", "tune"],
                     help="cg: the headline solve; cgm: the multi-shift workload; serve: the serving loop; "
                          "batched: 48 right-hand sides batched vs one at a time; configs: the 8^3x16 and "
                          "16^3x32 configurations with the reference's CPU solve; clover: the twisted-clover "
-                         "solve (extra reports)")
+                         "solve (extra reports); tune: the autotuner's choice and evidence per volume")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--requests", type=int, default=0, help="serve: number of requests")
     ap.add_argument("--serve-precision", default="single", choices=["double", "single", "half"])
+    ap.add_argument("--serve-priorities", type=int, default=0, choices=[0, 1],
+                    help="serve: give the streams of smaller volumes higher priorities")
     ap.add_argument("--cgm-precision", default="half", choices=["single", "half"])
     ap.add_argument("--precision", default="half", choices=["double", "single", "half"],
                     help="inner precision of the headline solve")
@@ -802,7 +858,7 @@ def main():
     if args.kernel_only:
         run_kernel_only(args)
         return
-    legs = {"cgm": leg_cgm, "serve": leg_serve, "batched": leg_batched, "configs": leg_configs}
+    legs = {"cgm": leg_cgm, "serve": leg_serve, "batched": leg_batched, "configs": leg_configs, "tune": leg_tune}
     if args.workload in legs:
         print(json.dumps(legs[args.workload](args)), flush=True)
         return

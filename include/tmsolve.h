@@ -321,7 +321,10 @@ int64_t tms_hop_stage_timeouts(tms_ctx *ctx);
  * neighbour spinors and links streamed through its own shared-memory slots by cp.async, three (FP32
  * spinors: two) directions ahead, 7 tiles of lattice rows whose neighbour faces and links are staged
  * in shared memory by bulk asynchronous copies before the same arithmetic (LZ a multiple of 8 and
- * 16-bit or FP32 12-real links, else shape 0 is used)),
+ * 16-bit or FP32 12-real links, else shape 0 is used)), "tma_rows" (the site tiling of shape 7: lattice
+ * rows of LZ/2 sites per tile, a divisor R of LY with R*LZ/2 <= 128 and either R == LY or R + 2 <= LY
+ * and R*LZ/2 >= 16; 0
+ * (default): the most that fit),
  * "graph_iters" (CG iterations per CUDA graph replay, 1..64), "reliable_delta_single",
  * "reliable_delta_half" (the mixed solvers recompute the FP64 residual when the iterated one has
  * dropped by this factor, 0 < delta < 1), "links_single" (0: the FP32-spinor inner solver reads FP32
@@ -337,6 +340,8 @@ int64_t tms_hop_stage_timeouts(tms_ctx *ctx);
  * "stream_priority" (the context's stream is recreated with this CUDA stream priority, an integer in the
  * device's range, lower first; contexts of small volumes sharing a GPU with large ones use it).  Results do not depend on the launch shapes. */
 tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);
+/* The current value of a tuning knob (the keys of tms_set_tuning). */
+tms_status tms_get_tuning(tms_ctx *ctx, const char *key, double *value);
 /* Time the e/o hopping kernel alone with CUDA events on the context's stream: nrep launches,
  * each preceded (untimed) by a 512 MiB write that flushes the L2 when flush=1.
  * precision: tms_precision; variant 0 plain hop, 1 hop + inverse diagonal (CG first half),

@@ -76,6 +76,7 @@ SIGNATURES = {
     "tms_launch_count": (ctypes.c_uint64, [P]),
     "tms_hop_stage_timeouts": (ctypes.c_int64, [P]),
     "tms_set_tuning": (I, [P, ctypes.c_char_p, D]),
+    "tms_get_tuning": (I, [P, ctypes.c_char_p, ctypes.POINTER(D)]),
     "tms_bench_hop": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),
     "tms_bench_hop_batched": (I, [P, I, I, I, I, ctypes.POINTER(D), ctypes.POINTER(D)]),
     "tms_hop_eo_noalloc": (I, [I, I, D, P, I, I, I, P, P, I, D, P, ctypes.c_char_p, I]),

@@ -101,7 +101,7 @@ tms_status tms_create4(tms_ctx** out, int T, int LX, int LY, int LZ, double bc_t
   };
   if (cudaSetDevice(device) != cudaSuccess) return cleanup(TMS_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return cleanup(TMS_ERR_CUDA);
-  ctx->red_cap = div_up(V, 64) + 1024;
+  ctx->red_cap = div_up(V, 16) + 1024; // block partials: a launch of at least 16 sites per block
   if (cudaMalloc(&ctx->lx_of_eo, sizeof(int) * V) != cudaSuccess ||
       cudaMalloc(&ctx->prm, sizeof(OpParams) * 2) != cudaSuccess ||
       cudaMalloc(&ctx->st, sizeof(CgState)) != cudaSuccess ||
@@ -437,6 +437,17 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       ctx->hop_cfg[p] = v;
       return TMS_OK;
     }
+  if (k == "tma_rows")
+    {
+      const int v = (int)value;
+      if (v != value || (v != 0 && !tma_rows_ok(ctx->g, v)))
+        return fail(ctx, TMS_ERR_BAD_ARG,
+                    "tma_rows: 0 or a divisor R of LY with R*LZ/2 <= %d and R == LY or R + 2 <= LY (LZ a multiple "
+                    "of 8)", HOP_TMA_THREADS);
+      if (ctx->tma_rows != v) drop_all();
+      ctx->tma_rows = v;
+      return TMS_OK;
+    }
   if (k == "graph_iters")
     {
       const int v = (int)value;
@@ -521,6 +532,34 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       return TMS_OK;
     }
   return fail(ctx, TMS_ERR_BAD_ARG, "unknown tuning key %s", key);
+}
+
+tms_status tms_get_tuning(tms_ctx* ctx, const char* key, double* value)
+{
+  if (!ctx || !key || !value) return TMS_ERR_BAD_ARG;
+  const std::string k = key;
+  if (k == "hop_cfg_double") *value = ctx->hop_cfg[PREC_F64];
+  else if (k == "hop_cfg_single") *value = ctx->hop_cfg[PREC_F32];
+  else if (k == "hop_cfg_half") *value = ctx->hop_cfg[PREC_F16];
+  else if (k == "tma_rows") *value = ctx->tma_rows;
+  else if (k == "graph_iters") *value = ctx->graph_iters;
+  else if (k == "batch_graph_iters") *value = ctx->batch_iters;
+  else if (k == "mrhs_per_thread") *value = ctx->mrhs_r;
+  else if (k == "links_single") *value = ctx->single_links16;
+  else if (k == "links_reliable") *value = ctx->reliable_links12;
+  else if (k == "reliable_delta_single") *value = ctx->delta_single;
+  else if (k == "reliable_delta_half") *value = ctx->delta_half;
+  else if (k == "pdl") *value = ctx->pdl;
+  else if (k == "cgm_floor_single") *value = ctx->cgm_floor32;
+  else if (k == "cgm_refine_batched") *value = ctx->cgm_refine_batched;
+  else if (k == "stream_priority")
+    {
+      int prio = 0;
+      CU(cudaStreamGetPriority(ctx->stream, &prio));
+      *value = prio;
+    }
+  else return fail(ctx, TMS_ERR_BAD_ARG, "unknown tuning key %s", key);
+  return TMS_OK;
 }
 
 tms_status tms_bench_hop(tms_ctx* ctx, int precision, int variant, int nrep, int flush, double* ms_per_launch,

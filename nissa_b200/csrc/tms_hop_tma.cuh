@@ -496,9 +496,19 @@ namespace tms
     if (Epi::kReduce) grid_reduce<HOP_TMA_THREADS>(part, red, fin);
   }
 
+  // a row count R the staged kernel can tile a (t, x) plane with: R divides LY,
+  // R LZ/2 sites fit the CTA, and a partial plane leaves room for its two halo
+  // rows and holds at least 16 sites (at most V/16 tiles: the reduction's capacity)
+  inline bool tma_rows_ok(const Lattice& g, int R)
+  {
+    return R >= 1 && g.LZ % 8 == 0 && g.LZ / 2 <= 64 && g.LY % R == 0 && R * (g.LZ / 2) <= HOP_TMA_THREADS &&
+           (R == g.LY || (R + 2 <= g.LY && R * (g.LZ / 2) >= 16));
+  }
+
   // the tile shape for a lattice, or ns = 0 when the staged kernel does not apply
-  // (LZ not a multiple of 8 or above 128, or no row count R dividing LY with R*LZ/2 <= the threads)
-  inline TmaGeom tma_geom(const Lattice& g, unsigned* timeouts)
+  // (LZ not a multiple of 8 or above 128, or no row count R dividing LY with R*LZ/2 <= the threads);
+  // rows > 0 asks for that many rows per tile (the site tiling), 0 for the most that fit
+  inline TmaGeom tma_geom(const Lattice& g, unsigned* timeouts, int rows = 0)
   {
     TmaGeom G{};
     G.timeouts = timeouts;
@@ -506,12 +516,14 @@ namespace tms
     G.LY = g.LY;
     G.NP = g.LY * G.h;
     if (g.LZ % 8 != 0 || G.h > 64) return G;
-    for (int R = g.LY; R >= 1; R--)
-      if (g.LY % R == 0 && R * G.h <= HOP_TMA_THREADS && (R == g.LY || R + 2 <= g.LY))
-        {
-          G.R = R;
-          break;
-        }
+    if (rows > 0 && tma_rows_ok(g, rows)) G.R = rows;
+    else
+      for (int R = g.LY; R >= 1; R--)
+        if (tma_rows_ok(g, R))
+          {
+            G.R = R;
+            break;
+          }
     if (G.R == 0) return G;
     G.ns = G.R * G.h;
     G.full = (G.R == g.LY);

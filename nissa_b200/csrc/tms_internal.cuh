@@ -139,6 +139,7 @@ struct tms_ctx
   // tuning (tms_set_tuning): hopping-kernel launch shape per precision, the
   // reliable-update trigger of the mixed solvers
   int hop_cfg[3] = {0, 1, 6};
+  int tma_rows = 0; // lattice rows per tile of the staged hop (launch shape 7): 0 the most that fit
   double delta_single = 1e-3, delta_half = 0.005;
   int single_links16 = 1; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
   int reliable_links12 = 1; // FP64 residuals of the mixed solvers on 12-real FP64 links (when SU(3) to rounding)
@@ -321,7 +322,7 @@ namespace tms_int
         if constexpr (LF == LINK_I16_12 || LF == LINK_F32_12)
           if (c->hop_cfg[P] == 7)
             {
-              const TmaGeom G = tma_geom(c->g, c->tma_timeouts);
+              const TmaGeom G = tma_geom(c->g, c->tma_timeouts, c->tma_rows);
               const int ntiles = G.ns ? (int)(npar * c->g.Vh / G.ns) : 0;
               if (G.ns && ntiles <= c->red_cap)
                 {

@@ -298,6 +298,13 @@ class Lattice:
         """Set a tuning knob of the C ABI (see tms_set_tuning in include/tmsolve.h)."""
         self._check(self.lib.tms_set_tuning(self.h, key.encode(), float(value)), "tms_set_tuning")
 
+    def get_tuning(self, key: str):
+        """Current value of a tuning knob (an int where the knob is integral)."""
+        v = ctypes.c_double()
+        self._check(self.lib.tms_get_tuning(self.h, key.encode(), ctypes.byref(v)), "tms_get_tuning")
+        return int(v.value) if v.value == int(v.value) and not key.startswith(("reliable_delta", "cgm_floor")) \
+            else v.value
+
     def bench_hop(self, precision="double", variant=0, nrep=20, flush=True):
         """Mean device time (ms) of one e/o hopping launch and its algorithmic bytes."""
         ms, by = ctypes.c_double(), ctypes.c_double()

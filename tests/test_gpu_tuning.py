@@ -48,6 +48,30 @@ def test_hop_shapes_agree(cuda_device, T, L, precision):
         assert lat.hop_stage_timeouts == 0
 
 
+@pytest.mark.parametrize("T,L", [(16, 8), (8, 16)])
+@pytest.mark.parametrize("precision", ["single", "half"])
+def test_tile_rows_agree(cuda_device, T, L, precision):
+    """The staged shape under every site tiling (rows per tile) solves to the
+    target and agrees with the FP64 solution; its waits never give up."""
+    from nissa_b200 import tune
+    conf = wl.gauge_conf(T, L, 0.35, seed=33)
+    src = wl.random_spinor(T * L ** 3 // 2, 9)
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        ref, st0 = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-22)
+        lat.set_tuning("hop_cfg_" + precision, tune.TILED_SHAPE)
+        rows = tune.tile_rows_choices(L, L)
+        assert rows
+        for key_, val, sol, st in _solve_all(lat, src, precision, [("tma_rows", r) for r in rows + [0]]):
+            assert st["true_rel_res2"] < 1e-20, (val, st)
+            assert rel(sol, ref) < 1e-8, val
+            assert st["iterations"] <= 1.1 * st0["iterations"] + 5, (val, st["iterations"], st0["iterations"])
+        assert lat.hop_stage_timeouts == 0
+        for bad in (3, L + 1, -1, 0.5):
+            with pytest.raises(TmError):
+                lat.set_tuning("tma_rows", bad)
+
+
 def test_full_lattice_packed(cuda_device):
     """The full-lattice operator (both parities in one launch) under the packed kernel."""
     T, L = 8, 4
@@ -71,6 +95,10 @@ def test_shape_range_checked(cuda_device):
             lat.set_tuning("hop_cfg_single", 8)
         lat.set_tuning("hop_cfg_half", 4)
         lat.set_tuning("hop_cfg_half", 7)
+        assert lat.get_tuning("hop_cfg_half") == 7 and lat.get_tuning("hop_cfg_single") == 1
+        assert lat.get_tuning("tma_rows") == 0 and lat.get_tuning("reliable_delta_half") == 0.005
+        with pytest.raises(TmError):
+            lat.get_tuning("no_such_knob")
 
 
 def test_autotune_on_device(cuda_device, tmp_path):
