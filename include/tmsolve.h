@@ -318,8 +318,8 @@ int64_t tms_hop_stage_timeouts(tms_ctx *ctx);
  * thread in packed FP32 arithmetic with the neighbours streamed through shared memory by cp.async,
  * 4 two sites per thread in packed FP32 arithmetic; for any T: 5 one site per thread with the two spin
  * rows of each half spinor in the lanes of packed FP32 arithmetic, 6 the same with each thread's
- * neighbour spinors and links streamed through its own shared-memory slots by cp.async, three (FP32
- * spinors: two) directions ahead, 7 tiles of lattice rows whose neighbour faces and links are staged
+ * neighbour spinors and links streamed through its own shared-memory slots by cp.async, two
+ * directions ahead, 7 tiles of lattice rows whose neighbour faces and links are staged
  * in shared memory by bulk asynchronous copies before the same arithmetic (LZ a multiple of 8 and
  * 16-bit or FP32 12-real links, else shape 0 is used)), "tma_rows" (the site tiling of shape 7: lattice
  * rows of LZ/2 sites per tile, a divisor R of LY with R*LZ/2 <= 128 and either R == LY or R + 2 <= LY

@@ -299,7 +299,7 @@ namespace tms
   template <int P>
   struct MrhsPipe
   {
-    static constexpr int DIST = (P == PREC_F16) ? 3 : 2;
+    static constexpr int DIST = 2;
   };
 
   template <int P, int LF, class Epi, class Fin, int R, bool PIPE = false>
