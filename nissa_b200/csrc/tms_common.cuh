@@ -12,8 +12,12 @@
 //   links,  FP32   float4  U[par][mu][3][Vh]        12 reals: rows 0 and 1; row 2 is
 //                                                   rebuilt as conj(row0 x row1)
 //   links,  FP32   float2  U[par][mu][9][Vh]        18 reals, for non-SU(3) links
-//   links,  I16    short4  U[par][mu][3][Vh]        12 reals in 16-bit fixed point (value/32767;
-//                                                   SU(3) entries are bounded by 1), row 2 rebuilt
+//   links,  I16    per (par, mu): uint4 U16[Vh], then uint2 U8[Vh]
+//                                                   12 reals in 16-bit fixed point (value/32767;
+//                                                   SU(3) entries are bounded by 1), row 2 rebuilt:
+//                                                   the first 8 of the 12 shorts in one 16-byte
+//                                                   word (copied past L1, no reuse), the last 4 in
+//                                                   one 8-byte word
 //
 // Sites of one parity are numbered as the reference numbers them
 // (geometry_eo.cpp:66-77): lx = ((t*LX + x)*LY + y)*LZ + z, and the e/o index
@@ -410,16 +414,28 @@ namespace tms
   template <> struct LinkT<LINK_I16_12>
   {
     using R = float;
-    const short4* __restrict__ d; // [par][mu][3][Vh]
+    // per (parity, direction) a block of two planes: shorts 0-7 of the two
+    // stored rows as one 16-byte word per site, shorts 8-11 as one 8-byte word
+    const char* __restrict__ d;
     int Vh;
     // stored rows 0 and 1 in raw 16-bit units (value = raw * kUnit), for the two-site kernels
     static constexpr int kRows = 2;
     static constexpr float kUnit = 1.0f / 32767.0f;
-    template <bool STREAM = true>
-    __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[6]) const
+    // bytes of one (parity, direction) block: 24 per site, kept a multiple of 16
+    __host__ __device__ static size_t block_bytes(int64_t Vh) { return ((size_t)24 * Vh + 15) & ~(size_t)15; }
+    __device__ __forceinline__ const uint4* w16(int par, int mu) const
     {
-      const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const short4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
+      return reinterpret_cast<const uint4*>(d + (size_t)(par * 4 + mu) * block_bytes(Vh));
+    }
+    __device__ __forceinline__ const uint2* w8(int par, int mu) const
+    {
+      return reinterpret_cast<const uint2*>(d + (size_t)(par * 4 + mu) * block_bytes(Vh) + (size_t)16 * Vh);
+    }
+    // the twelve stored shorts of a link (16-byte word a, 8-byte word b) as rows 0 and 1
+    __device__ __forceinline__ static void decode_raw(const uint4& a, const uint2& b, C<float> u[6])
+    {
+      const short4 a0 = *reinterpret_cast<const short4*>(&a.x), a1 = *reinterpret_cast<const short4*>(&a.z);
+      const short4 a2 = *reinterpret_cast<const short4*>(&b);
       u[0] = {float(a0.x), float(a0.y)};
       u[1] = {float(a0.z), float(a0.w)};
       u[2] = {float(a1.x), float(a1.y)};
@@ -427,20 +443,18 @@ namespace tms
       u[4] = {float(a2.x), float(a2.y)};
       u[5] = {float(a2.z), float(a2.w)};
     }
+    template <bool STREAM = true>
+    __device__ __forceinline__ void load_rows(int par, int mu, int site, C<float> u[6]) const
+    {
+      decode_raw(ld_link<STREAM>(w16(par, mu) + site), ld_link<STREAM>(w8(par, mu) + site), u);
+    }
     // rows 0 and 1 in raw 16-bit units, row 2 rebuilt from them and brought to
     // the same units: the products of this link are to be multiplied by `scale`
     template <bool STREAM = true>
     __device__ __forceinline__ void load_scaled(int par, int mu, int site, C<float> u[9], float& scale) const
     {
       constexpr float k = 1.0f / 32767.0f;
-      const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const short4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
-      u[0] = {float(a0.x), float(a0.y)};
-      u[1] = {float(a0.z), float(a0.w)};
-      u[2] = {float(a1.x), float(a1.y)};
-      u[3] = {float(a1.z), float(a1.w)};
-      u[4] = {float(a2.x), float(a2.y)};
-      u[5] = {float(a2.z), float(a2.w)};
+      load_rows<STREAM>(par, mu, site, u);
       u[6] = cscale(cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4]))), k);
       u[7] = cscale(cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5]))), k);
       u[8] = cscale(cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3]))), k);
@@ -450,14 +464,9 @@ namespace tms
     __device__ __forceinline__ void load(int par, int mu, int site, C<float> u[9]) const
     {
       constexpr float k = 1.0f / 32767.0f;
-      const short4* b = d + ((size_t)(par * 4 + mu) * 3) * Vh + site;
-      const short4 a0 = ld_link<STREAM>(b), a1 = ld_link<STREAM>(b + Vh), a2 = ld_link<STREAM>(b + 2 * (size_t)Vh);
-      u[0] = {a0.x * k, a0.y * k};
-      u[1] = {a0.z * k, a0.w * k};
-      u[2] = {a1.x * k, a1.y * k};
-      u[3] = {a1.z * k, a1.w * k};
-      u[4] = {a2.x * k, a2.y * k};
-      u[5] = {a2.z * k, a2.w * k};
+      load_rows<STREAM>(par, mu, site, u);
+#pragma unroll
+      for (int c = 0; c < 6; c++) u[c] = {u[c].re * k, u[c].im * k};
       u[6] = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
       u[7] = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));
       u[8] = cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));

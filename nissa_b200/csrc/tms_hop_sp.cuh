@@ -229,7 +229,7 @@ namespace tms
 // ---------------------------------------------------------------------------
 // The same one-site packed kernel with the neighbours' data streamed into the
 // thread's own shared-memory slots by cp.async, DIST directions ahead of the
-// direction it computes (launch shape 6; DIST = 3 for FP16 spinors, 2 for FP32).  The gather needs many loads in
+// direction it computes (launch shape 6, DIST = 2).  The gather needs many loads in
 // flight; in registers they cost occupancy, in shared memory they cost
 // nothing while the arithmetic of the earlier directions runs.  A thread reads
 // back only what it copied itself, so the only synchronisation is
@@ -247,8 +247,8 @@ namespace tms
   {
     static constexpr int KS = (P == PREC_F16) ? 3 : 6;                                 // spinor, 16-byte words
     static constexpr int HASN = (P == PREC_F16) ? 1 : 0;                               // FP16 per-site factor
-    static constexpr int KL16 = (LF == LINK_F32_12) ? 3 : 0;                           // link, 16-byte words
-    static constexpr int KL8 = (LF == LINK_I16_12) ? 3 : (LF == LINK_F32_18) ? 9 : 0; // link, 8-byte words
+    static constexpr int KL16 = (LF == LINK_F32_12) ? 3 : (LF == LINK_I16_12) ? 1 : 0;    // link, 16-byte words
+    static constexpr int KL8 = (LF == LINK_I16_12) ? 1 : (LF == LINK_F32_18) ? 9 : 0;     // link, 8-byte words
     static constexpr int W16 = KS + KL16;
     static constexpr int SLOT_BYTES = W16 * 16 + KL8 * 8 + HASN * 4;
     template <int DIST>
@@ -289,17 +289,26 @@ namespace tms
 #pragma unroll
     for (int k = 0; k < F::KS; k++) cp_async16(sl.w16(slot, k), sp + (size_t)k * in.stride + n);
     if (F::HASN) cp_async4(sl.nrm(slot), in.n + n);
-    if (F::KL16)
+    if constexpr (LF == LINK_I16_12)
       {
-        const uint4* b = reinterpret_cast<const uint4*>(U.d) + ((size_t)(lpar * 4 + MU) * 3) * U.Vh + ls;
-#pragma unroll
-        for (int k = 0; k < F::KL16; k++) cp_async16_stream(sl.w16(slot, F::KS + k), b + (size_t)k * U.Vh);
+        // the 16-byte word past L1 (a link is read once), the 8-byte word through it
+        cp_async16_stream(sl.w16(slot, F::KS), U.w16(lpar, MU) + ls);
+        cp_async8(sl.w8(slot, 0), U.w8(lpar, MU) + ls);
       }
-    if (F::KL8)
+    else
       {
-        const uint2* b = reinterpret_cast<const uint2*>(U.d) + ((size_t)(lpar * 4 + MU) * F::KL8) * U.Vh + ls;
+        if (F::KL16)
+          {
+            const uint4* b = reinterpret_cast<const uint4*>(U.d) + ((size_t)(lpar * 4 + MU) * 3) * U.Vh + ls;
 #pragma unroll
-        for (int k = 0; k < F::KL8; k++) cp_async8(sl.w8(slot, k), b + (size_t)k * U.Vh);
+            for (int k = 0; k < F::KL16; k++) cp_async16_stream(sl.w16(slot, F::KS + k), b + (size_t)k * U.Vh);
+          }
+        if (F::KL8)
+          {
+            const uint2* b = reinterpret_cast<const uint2*>(U.d) + ((size_t)(lpar * 4 + MU) * F::KL8) * U.Vh + ls;
+#pragma unroll
+            for (int k = 0; k < F::KL8; k++) cp_async8(sl.w8(slot, k), b + (size_t)k * U.Vh);
+          }
       }
   }
 
@@ -336,24 +345,11 @@ namespace tms
             v[2 * k + 1] = {f.z, f.w};
           }
       }
-    if (LF == LINK_I16_12)
+    if constexpr (LF == LINK_I16_12)
       {
-        constexpr float k = 1.0f / 32767.0f;
-        short4 a[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-          {
-            const uint2 w = *sl.w8(slot, r);
-            a[r] = *reinterpret_cast<const short4*>(&w);
-          }
-        u[0] = {float(a[0].x), float(a[0].y)};
-        u[1] = {float(a[0].z), float(a[0].w)};
-        u[2] = {float(a[1].x), float(a[1].y)};
-        u[3] = {float(a[1].z), float(a[1].w)};
-        u[4] = {float(a[2].x), float(a[2].y)};
-        u[5] = {float(a[2].z), float(a[2].w)};
+        LinkT<LINK_I16_12>::decode_raw(*sl.w16(slot, SppFmt<P, LF>::KS), *sl.w8(slot, 0), u);
         row2_unscaled(u); // in raw^2 units: sp_dir_compute scales its products by k
-        ls = k;
+        ls = 1.0f / 32767.0f;
       }
     else if (LF == LINK_F32_12)
       {

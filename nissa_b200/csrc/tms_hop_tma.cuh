@@ -106,32 +106,29 @@ namespace tms
   template <int LF> struct StageLk;
   template <> struct StageLk<LINK_I16_12>
   {
-    static constexpr int NC = 3;  // planes per (parity, direction)
-    static constexpr int ES = 8;  // bytes per site of a plane
+    static constexpr int NC = 2;  // planes per (parity, direction): the 16-byte and the 8-byte word
+    static constexpr int KB = 24; // bytes per site of all planes
+    __device__ static int es(int c) { return c ? 8 : 16; }
+    __device__ static int off(int c) { return c ? 16 : 0; } // bytes per site before plane c
     __device__ static const char* src(const LinkT<LINK_I16_12>& U, int par, int mu, int c)
     {
-      return reinterpret_cast<const char*>(U.d + ((size_t)(par * 4 + mu) * 3 + c) * U.Vh);
+      return c ? reinterpret_cast<const char*>(U.w8(par, mu)) : reinterpret_cast<const char*>(U.w16(par, mu));
     }
     // the link of slot q: raw rows 0 and 1, row 2 rebuilt in raw^2 units
     __device__ static void load(const char* base, int nslots, int q, C<float> u[9], float& scale)
     {
-      const short4* b = reinterpret_cast<const short4*>(base);
-      const short4 a0 = b[q], a1 = b[nslots + q], a2 = b[2 * nslots + q];
-      constexpr float k = 1.0f / 32767.0f;
-      u[0] = {float(a0.x), float(a0.y)};
-      u[1] = {float(a0.z), float(a0.w)};
-      u[2] = {float(a1.x), float(a1.y)};
-      u[3] = {float(a1.z), float(a1.w)};
-      u[4] = {float(a2.x), float(a2.y)};
-      u[5] = {float(a2.z), float(a2.w)};
+      LinkT<LINK_I16_12>::decode_raw(reinterpret_cast<const uint4*>(base)[q],
+                                     reinterpret_cast<const uint2*>(base + (size_t)16 * nslots)[q], u);
       row2_unscaled(u); // raw^2 units: the arithmetic scales row 2's products by k
-      scale = k;
+      scale = 1.0f / 32767.0f;
     }
   };
   template <> struct StageLk<LINK_F32_12>
   {
     static constexpr int NC = 3;
-    static constexpr int ES = 16;
+    static constexpr int KB = 48;
+    __device__ static int es(int) { return 16; }
+    __device__ static int off(int c) { return 16 * c; }
     __device__ static const char* src(const LinkT<LINK_F32_12>& U, int par, int mu, int c)
     {
       return reinterpret_cast<const char*>(U.d + ((size_t)(par * 4 + mu) * 3 + c) * U.Vh);
@@ -211,7 +208,7 @@ namespace tms
     // link buffers: forward mu (f = 0..3), backward mu (f = 4..7)
     __device__ size_t links(int f) const
     {
-      return (size_t)(nc + 4 * ns) * StageSp<P>::kBytes + (size_t)f * ns * StageLk<LF>::NC * StageLk<LF>::ES;
+      return (size_t)(nc + 4 * ns) * StageSp<P>::kBytes + (size_t)f * ns * StageLk<LF>::KB;
     }
   };
 
@@ -296,7 +293,7 @@ namespace tms
         return CopyDesc{dst, base + (size_t)src_site * es, (unsigned)(nsites * es)};
       }
     q -= StageSp<P>::NC * nsp;
-    constexpr int NCL = StageLk<LF>::NC, ESL = StageLk<LF>::ES;
+    constexpr int NCL = StageLk<LF>::NC;
     const int tile0 = plane * NP + r0 * h; // first site of the tile
     int par, mu, c, src_site, nsites;
     size_t dst;
@@ -308,7 +305,7 @@ namespace tms
         par = p;
         src_site = tile0;
         nsites = G.ns;
-        dst = lay.links(mu) + (size_t)c * G.ns * ESL;
+        dst = lay.links(mu) + (size_t)G.ns * StageLk<LF>::off(c);
       }
     else
       {
@@ -321,7 +318,7 @@ namespace tms
             c = q;
             src_site = tile0;
             nsites = G.ns;
-            dst = lay.links(4 + 3) + (size_t)c * G.ns * ESL;
+            dst = lay.links(4 + 3) + (size_t)G.ns * StageLk<LF>::off(c);
           }
         else if (q < 3 * NCL)
           {
@@ -329,7 +326,7 @@ namespace tms
             mu = 2;
             q -= NCL;
             c = q >> 1;
-            const size_t cb = lay.links(4 + 2) + (size_t)c * G.ns * ESL;
+            const size_t cb = lay.links(4 + 2) + (size_t)G.ns * StageLk<LF>::off(c);
             if ((q & 1) == 0)
               {
                 src_site = plane * NP + ((r0 - 1 + LY) % LY) * h;
@@ -340,7 +337,7 @@ namespace tms
               {
                 src_site = tile0;
                 nsites = (R - 1) * h;
-                dst = cb + (size_t)h * ESL;
+                dst = cb + (size_t)h * StageLk<LF>::es(c);
               }
           }
         else if (q < 4 * NCL)
@@ -350,7 +347,7 @@ namespace tms
             c = q - 3 * NCL;
             src_site = (t * g.LX + (x - 1 + g.LX) % g.LX) * NP + r0 * h;
             nsites = G.ns;
-            dst = lay.links(4 + 1) + (size_t)c * G.ns * ESL;
+            dst = lay.links(4 + 1) + (size_t)G.ns * StageLk<LF>::off(c);
           }
         else
           {
@@ -359,10 +356,11 @@ namespace tms
             c = q - 4 * NCL;
             src_site = (((t - 1 + g.T) % g.T) * g.LX + x) * NP + r0 * h;
             nsites = G.ns;
-            dst = lay.links(4 + 0) + (size_t)c * G.ns * ESL;
+            dst = lay.links(4 + 0) + (size_t)G.ns * StageLk<LF>::off(c);
           }
       }
-    return CopyDesc{dst, StageLk<LF>::src(U, par, mu, c) + (size_t)src_site * ESL, (unsigned)(nsites * ESL)};
+    const int esl = StageLk<LF>::es(c);
+    return CopyDesc{dst, StageLk<LF>::src(U, par, mu, c) + (size_t)src_site * esl, (unsigned)(nsites * esl)};
   }
 
   // bytes the tile's copies deliver (the barrier's transaction count)
@@ -370,7 +368,7 @@ namespace tms
   __device__ __forceinline__ unsigned tma_tile_bytes(const TmaGeom& G)
   {
     return (unsigned)((size_t)(G.nc + 4 * G.ns) * StageSp<P>::kBytes +
-                      (size_t)8 * G.ns * StageLk<LF>::NC * StageLk<LF>::ES);
+                      (size_t)8 * G.ns * StageLk<LF>::KB);
   }
 
   // one direction of the stencil from the staged data

@@ -62,7 +62,7 @@ struct tms_ctx
   double2* U64 = nullptr;
   float4* U32r = nullptr; // 12-real
   float2* U32f = nullptr; // 18-real
-  short4* U16r = nullptr; // 12-real, 16-bit fixed point
+  char* U16r = nullptr; // 12-real, 16-bit fixed point (LinkT<LINK_I16_12> blocks)
 
   // scalars and reduction scratch
   OpParams* prm = nullptr;       // [2]: operator params (slot 0 solver, slot 1 free use)
@@ -418,7 +418,7 @@ namespace tms_int
 
   // FP32 copies and the special-unitarity check (max deviation over links)
   static __global__ void conf_lowprec_kernel(int64_t nlinks_per_parmu, int Vh, const double2* __restrict__ U,
-                                      float4* __restrict__ Ur, float2* __restrict__ Uf, short4* __restrict__ Us,
+                                      float4* __restrict__ Ur, float2* __restrict__ Uf, char* __restrict__ Us,
                                       Reducer red)
   {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; // over 8*Vh (par,mu,site)
@@ -437,9 +437,18 @@ namespace tms_int
         Ur[((size_t)pm * 3 + 1) * Vh + site] = make_float4((float)u[2].re, (float)u[2].im, (float)u[3].re, (float)u[3].im);
         Ur[((size_t)pm * 3 + 2) * Vh + site] = make_float4((float)u[4].re, (float)u[4].im, (float)u[5].re, (float)u[5].im);
         auto q = [](double x) { return (short)__double2int_rn(fmin(1.0, fmax(-1.0, x)) * 32767.0); };
-        Us[((size_t)pm * 3 + 0) * Vh + site] = make_short4(q(u[0].re), q(u[0].im), q(u[1].re), q(u[1].im));
-        Us[((size_t)pm * 3 + 1) * Vh + site] = make_short4(q(u[2].re), q(u[2].im), q(u[3].re), q(u[3].im));
-        Us[((size_t)pm * 3 + 2) * Vh + site] = make_short4(q(u[4].re), q(u[4].im), q(u[5].re), q(u[5].im));
+        {
+          // the LinkT<LINK_I16_12> block of (par, mu): shorts 0-7 as a 16-byte word, 8-11 as an 8-byte word
+          const short4 a0 = make_short4(q(u[0].re), q(u[0].im), q(u[1].re), q(u[1].im));
+          const short4 a1 = make_short4(q(u[2].re), q(u[2].im), q(u[3].re), q(u[3].im));
+          const short4 a2 = make_short4(q(u[4].re), q(u[4].im), q(u[5].re), q(u[5].im));
+          char* blk = Us + (size_t)pm * LinkT<LINK_I16_12>::block_bytes(Vh);
+          uint4 w;
+          memcpy(&w.x, &a0, 8);
+          memcpy(&w.z, &a1, 8);
+          reinterpret_cast<uint4*>(blk)[site] = w;
+          reinterpret_cast<short4*>(blk + (size_t)16 * Vh)[site] = a2;
+        }
         // deviation of row 2 from conj(row0 x row1), plus row-0/1 unitarity
         const C<double> c0 = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
         const C<double> c1 = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));

@@ -26,8 +26,8 @@ namespace tms
   {
     static constexpr int KS16 = (P == PREC_F16) ? 3 : 6;                                 // spinor, 16-byte words
     static constexpr int HASN = (P == PREC_F16) ? 1 : 0;                                 // FP16 per-site factor
-    static constexpr int KL16 = (LF == LINK_F32_12) ? 3 : 0;                             // link, 16-byte words
-    static constexpr int KL8 = (LF == LINK_I16_12) ? 3 : (LF == LINK_F32_18) ? 9 : 0;  // link, 8-byte words
+    static constexpr int KL16 = (LF == LINK_F32_12) ? 3 : (LF == LINK_I16_12) ? 1 : 0;   // link, 16-byte words
+    static constexpr int KL8 = (LF == LINK_I16_12) ? 1 : (LF == LINK_F32_18) ? 9 : 0;    // link, 8-byte words
     static constexpr int W16 = KS16 + KL16;
     // directions in flight + 1 (fewer for FP32 spinors, to keep two blocks per SM)
     static constexpr int SLOTS = (P == PREC_F16) ? 4 : 3;
@@ -103,17 +103,26 @@ namespace tms
 #pragma unroll
         for (int k = 0; k < F::KS16; k++) cp_async16(sm.w16(slot, j, k), sp + (size_t)k * in.stride + n);
         if (F::HASN) cp_async4(sm.nrm(slot, j), in.n + n);
-        if (F::KL16)
+        if constexpr (LF == LINK_I16_12)
           {
-            const uint4* b = reinterpret_cast<const uint4*>(U.d) + ((size_t)(lpar * 4 + MU) * 3) * U.Vh + ls;
-#pragma unroll
-            for (int k = 0; k < F::KL16; k++) cp_async16_stream(sm.w16(slot, j, F::KS16 + k), b + (size_t)k * U.Vh);
+            cp_async16_stream(sm.w16(slot, j, F::KS16), U.w16(lpar, MU) + ls);
+            cp_async8(sm.w8(slot, j, 0), U.w8(lpar, MU) + ls);
           }
-        if (F::KL8)
+        else
           {
-            const uint2* b = reinterpret_cast<const uint2*>(U.d) + ((size_t)(lpar * 4 + MU) * F::KL8) * U.Vh + ls;
+            if (F::KL16)
+              {
+                const uint4* b = reinterpret_cast<const uint4*>(U.d) + ((size_t)(lpar * 4 + MU) * 3) * U.Vh + ls;
 #pragma unroll
-            for (int k = 0; k < F::KL8; k++) cp_async8(sm.w8(slot, j, k), b + (size_t)k * U.Vh);
+                for (int k = 0; k < F::KL16; k++)
+                  cp_async16_stream(sm.w16(slot, j, F::KS16 + k), b + (size_t)k * U.Vh);
+              }
+            if (F::KL8)
+              {
+                const uint2* b = reinterpret_cast<const uint2*>(U.d) + ((size_t)(lpar * 4 + MU) * F::KL8) * U.Vh + ls;
+#pragma unroll
+                for (int k = 0; k < F::KL8; k++) cp_async8(sm.w8(slot, j, k), b + (size_t)k * U.Vh);
+              }
           }
       }
   }
@@ -167,16 +176,8 @@ namespace tms
             u[2 * k + 1] = {w.z, w.w};
           }
       }
-    else if (LF == LINK_I16_12)
-      {
-#pragma unroll
-        for (int k = 0; k < 3; k++)
-          {
-            const short4 w = *reinterpret_cast<const short4*>(sm.w8(slot, j, k));
-            u[2 * k] = {float(w.x), float(w.y)};
-            u[2 * k + 1] = {float(w.z), float(w.w)};
-          }
-      }
+    else if constexpr (LF == LINK_I16_12)
+      LinkT<LINK_I16_12>::decode_raw(*sm.w16(slot, j, F::KS16), *sm.w8(slot, j, 0), u);
     else
       {
 #pragma unroll
