@@ -824,7 +824,7 @@ def run_clover(args):
 
 
 SERVE_WORKLOAD = dict(volumes={"8^3x16": (16, 8), "16^3x32": (32, 16), "32^3x64": (64, 32)},
-                      probs=[0.5, 0.35, 0.15], eps=0.35, seed=1, rate=20.0, requests=200, nslots=16)
+                      probs=[0.5, 0.35, 0.15], eps=0.35, seed=1, rate=20.0, requests=400, nslots=16)
 
 
 def leg_serve(args):

@@ -339,6 +339,9 @@ namespace tms
                 const Site s = eo_site(g, par_out, ieo);
                 if constexpr (PIPE && P != PREC_F64 && R == 1)
                   {
+                    // (the epilogue's operands are read from global memory here: staging them in
+                    // the free pipeline slots, as the single-RHS kernel does, made the whole batched
+                    // solve 7.7 % slower, although each launch timed alone was faster)
                     C<float> acc[12];
                     spp_hop_site<P, LF, MrhsPipe<P>::DIST>(mrhs_smem, g, par_out, ieo, in.rhs(rhs0), U, float(anis),
                                                            acc);

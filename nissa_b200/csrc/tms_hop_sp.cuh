@@ -391,13 +391,63 @@ namespace tms
     sp_dir_compute<MU, (D % 2) == 0, LF == LINK_I16_12>(sp, L, f, A01, A23, 1.0f / 32767.0f);
   }
 
+  // an FP16 field at site `site` into a slot's spinor words (an epilogue operand)
+  template <int P, int LF, int SLOTS>
+  __device__ __forceinline__ void spp_stage(const SppSlots<P, LF, SLOTS>& sl, int slot, const SpinorT<P>& f, int site)
+  {
+    const uint4* sp = reinterpret_cast<const uint4*>(f.d);
+#pragma unroll
+    for (int k = 0; k < 3; k++) cp_async16(sl.w16(slot, k), sp + (size_t)k * f.stride + site);
+    cp_async4(sl.nrm(slot), f.n + site);
+  }
+
+  // The loader an epilogue gets from the pipelined hop: operand k < n is read
+  // from slot (8 + k) % SLOTS, where the hop staged it (the same arithmetic as
+  // SpinorT<PREC_F16>::load), any other from global memory.
+  template <int P, int LF, int SLOTS>
+  struct SppStagedLoad
+  {
+    SppSlots<P, LF, SLOTS> sl;
+    int n;
+    template <int Q>
+    __device__ __forceinline__ void operator()(int k, const SpinorT<Q>& f, int site,
+                                               C<typename SpinorT<Q>::R> v[12]) const
+    {
+      if constexpr (Q == PREC_F16)
+        if (k < n)
+          {
+            const int slot = (8 + k) % SLOTS;
+            const float s = *sl.nrm(slot);
+#pragma unroll
+            for (int w = 0; w < 3; w++)
+              {
+                const uint4 x = *sl.w16(slot, w);
+                const unsigned u[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                  {
+                    const float2 h = __half22float2(*reinterpret_cast<const __half2*>(&u[j]));
+                    v[4 * w + j] = {h.x * s, h.y * s};
+                  }
+              }
+            return;
+          }
+      f.load(site, v);
+    }
+  };
+
   // the hop of site (p, ieo) with the thread's gathers pipelined through its
   // slots of `smem` (SppFmt::smem<DIST>() bytes for the block), in the
-  // accumulator layout of hop_site
-  template <int P, int LF, int DIST>
+  // accumulator layout of hop_site.  With nstaged > 0 (at most DIST), the
+  // FP16 fields staged[k] at the site itself are copied into the slots freed
+  // by the last directions (for the epilogue: SppStagedLoad), and have landed
+  // on return.
+  template <int P, int LF, int DIST, int NSTAGED = 0>
   __device__ __forceinline__ void spp_hop_site(char* smem, const Lattice& g, int p, int ieo, const SpinorT<P>& in,
-                                               const LinkT<LF>& U, float anis, C<float> acc[12])
+                                               const LinkT<LF>& U, float anis, C<float> acc[12],
+                                               const SpinorT<P>* staged = nullptr)
   {
+    static_assert(NSTAGED <= DIST && (NSTAGED == 0 || P == PREC_F16), "operands staged in the free slots");
     constexpr int SLOTS = DIST + 1;
     const SppSlots<P, LF, SLOTS> sl{smem, (int)(threadIdx.x % SPP_THREADS)};
     const Site s = eo_site(g, p, ieo);
@@ -412,6 +462,7 @@ namespace tms
     // the copies of the first DIST directions, one commit group each
 #define TMS_SPP_ISSUE(D)                                                                                           \
   if ((D) < 8) spp_issue<((D) < 8 ? (D) : 0), P, LF, SLOTS>(sl, (D) % SLOTS, g, s, p, ieo, in, U, w[(D) < 8 ? (D) : 0]); \
+  else if ((D) - 8 < NSTAGED) spp_stage(sl, (D) % SLOTS, staged[(D) >= 8 ? (D) - 8 : 0], ieo);                  \
   cp_async_commit();
 #define TMS_SPP_STEP(D)                                                                                            \
   TMS_SPP_ISSUE((D) + DIST)                                                                                        \
@@ -430,6 +481,7 @@ namespace tms
     TMS_SPP_STEP(7)
 #undef TMS_SPP_STEP
 #undef TMS_SPP_ISSUE
+    if (NSTAGED > 0) cp_async_wait<0>();
 #pragma unroll
     for (int c = 0; c < 3; c++)
       {
@@ -460,8 +512,22 @@ namespace tms
     if (active)
       {
         C<float> acc[12];
-        spp_hop_site<P, LF, DIST>(spp_smem, g, p, ieo, p ? in_e : in_o, U, float(prm->anis), acc);
-        part = epi(p, ieo, acc);
+        // the epilogue's FP16 operands ride in the slots the last directions free
+        constexpr int NS = (P == PREC_F16) ? (EpiStaged<Epi>::n < DIST ? EpiStaged<Epi>::n : DIST) : 0;
+        if constexpr (NS > 0)
+          {
+            SpinorT<P> stg[NS];
+#pragma unroll
+            for (int k = 0; k < NS; k++) stg[k] = epi.staged(p, k);
+            spp_hop_site<P, LF, DIST, NS>(spp_smem, g, p, ieo, p ? in_e : in_o, U, float(prm->anis), acc, stg);
+            part = epi.run(p, ieo, acc,
+                           SppStagedLoad<P, LF, DIST + 1>{{spp_smem, (int)(threadIdx.x % SPP_THREADS)}, NS});
+          }
+        else
+          {
+            spp_hop_site<P, LF, DIST>(spp_smem, g, p, ieo, p ? in_e : in_o, U, float(prm->anis), acc);
+            part = epi(p, ieo, acc);
+          }
       }
     if (Epi::kReduce) grid_reduce<SPP_THREADS>(part, red, fin);
   }

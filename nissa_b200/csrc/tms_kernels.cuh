@@ -92,6 +92,30 @@ namespace tms
     return r;
   }
 
+  // Epilogue operand loads go through a loader, ld(k, field, site, v): operand
+  // k of the output site.  The plain one reads global memory; the pipelined
+  // hops pass one that reads the operands they staged in shared memory while
+  // the last directions were computed (the first EpiStaged<E>::n operands,
+  // whose fields the epilogue names with staged()).
+  struct LoadGlobal
+  {
+    template <int P>
+    __device__ __forceinline__ void operator()(int, const SpinorT<P>& f, int site, C<typename SpinorT<P>::R> v[12]) const
+    {
+      f.load(site, v);
+    }
+  };
+  template <class E, class = void>
+  struct EpiStaged
+  {
+    static constexpr int n = 0;
+  };
+  template <class E>
+  struct EpiStaged<E, decltype((void)E::kStaged)>
+  {
+    static constexpr int n = E::kStaged;
+  };
+
   // ------------------------------------------------------- stencil body
   // Accumulates the -2*hopping term sum_mu [(1-g_mu) U_x,mu in(x+mu) + (1+g_mu) U^+_x-mu,mu in(x-mu)]
   // in the reference's chiral basis; projection and reconstruction tables follow
@@ -294,16 +318,23 @@ namespace tms
   struct EpiKern
   {
     static constexpr bool kReduce = RED;
+    static constexpr int kStaged = (P == PREC_F16) ? 1 : 0; // x
     SpinorT<P> out[2];
     SpinorT<P> x[2];
     const OpParams* prm;
     double sgn;
+    __device__ __forceinline__ SpinorT<P> staged(int p, int) const { return pick(x[0], x[1], p); }
     __device__ __forceinline__ double operator()(int p, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      return run(p, ieo, acc, LoadGlobal{});
+    }
+    template <class LD>
+    __device__ __forceinline__ double run(int p, int ieo, C<typename SpinorT<P>::R> acc[12], const LD& ld) const
     {
       using R = typename SpinorT<P>::R;
       const C<R> z = zdiag<R>(*prm, sgn);
       C<R> xv[12];
-      pick(x[0], x[1], p).load(ieo, xv);
+      ld(0, pick(x[0], x[1], p), ieo, xv);
       double n2 = 0.0;
 #pragma unroll
       for (int c = 0; c < 12; c++)
@@ -494,6 +525,7 @@ namespace tms
   struct EpiKernCgUpdate
   {
     static constexpr bool kReduce = true;
+    static constexpr int kStaged = (P == PREC_F16) ? 2 : 0; // t1, r
     SpinorT<P> t1;    // the input of K(+mu) at the output site
     SpinorT<P> r, p;
     SpinorT<PX> x;
@@ -501,14 +533,20 @@ namespace tms
     const CgState* st;
     double sgn;
     SpinorT<P> pp;    // XM == 2: the previous direction
+    __device__ __forceinline__ SpinorT<P> staged(int, int k) const { return k ? r : t1; }
     __device__ __forceinline__ double operator()(int par, int ieo, C<typename SpinorT<P>::R> acc[12]) const
+    {
+      return run(par, ieo, acc, LoadGlobal{});
+    }
+    template <class LD>
+    __device__ __forceinline__ double run(int par, int ieo, C<typename SpinorT<P>::R> acc[12], const LD& ld) const
     {
       using R = typename SpinorT<P>::R;
       using RX = typename SpinorT<PX>::R;
       const C<R> z = zdiag<R>(*prm, sgn);
       const R alpha = R(st->alpha);
       C<R> v[12];
-      t1.load(ieo, v);
+      ld(0, t1, ieo, v);
 #pragma unroll
       for (int c = 0; c < 12; c++)
         {
@@ -516,7 +554,7 @@ namespace tms
           const C<R> q = cscale(acc[c], R(0.25));
           acc[c] = (c < 6) ? csub(d, q) : csub(q, d); // s
         }
-      r.load(ieo, v);
+      ld(1, r, ieo, v);
       double n2 = 0.0;
 #pragma unroll
       for (int c = 0; c < 12; c++)

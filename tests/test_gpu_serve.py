@@ -15,10 +15,11 @@ from conftest import rel
 pytestmark = pytest.mark.gpu
 
 
-def test_mix_equals_alone(cuda_device):
+@pytest.mark.parametrize("precision", ["single", "half"])
+def test_mix_equals_alone(cuda_device, precision):
     vols = {"4^4": (4, 4, wl.gauge_conf(4, 4, 0.35, 81)), "8^3x8": (8, 8, wl.gauge_conf(8, 8, 0.35, 82)),
             "8^3x16": (16, 8, wl.gauge_conf(16, 8, 0.35, 83))}
-    res = GpuResidency(vols, nslots=4, precision="single")
+    res = GpuResidency(vols, nslots=4, precision=precision)
     srv = SolveServer(res.backends(), free_memory=res.free_memory)
     sched = poisson_requests(16, rate=400.0, volumes=list(vols), probs=[0.5, 0.35, 0.15], seed=7)
     results, wall = run_load(srv, sched, timeout=600)
@@ -31,7 +32,7 @@ def test_mix_equals_alone(cuda_device):
         assert r.stats["true_rel_res2"] < q.residue
         lat = res.lattices[q.volume]
         src = res.make_source(q.volume, q)
-        alone, st = lat.inv_tmD_cg_eoprec(q.kappa, q.mu, src, 100000, q.residue, precision="single")
+        alone, st = lat.inv_tmD_cg_eoprec(q.kappa, q.mu, src, 100000, q.residue, precision=precision)
         err = rel(r.solution.cpu().numpy(), alone.cpu().numpy())
         assert err < 100 * math.sqrt(q.residue), (q, err)
     res.close()
