@@ -841,10 +841,10 @@ def leg_serve(args):
                        priorities=bool(args.serve_priorities))
     srv = SolveServer(res.backends(), free_memory=res.free_memory, reserve_bytes=2 << 30)
     warm = poisson_requests(6, rate=100.0, volumes=list(vols), probs=[1 / 3] * 3, seed=99)
-    run_load(srv, warm)
+    run_load(srv, warm, keep_solutions=False)
     sched = poisson_requests(n, rate=rate, volumes=list(vols), probs=W["probs"], seed=W["seed"])
     with ClockSampler(0) as clk:
-        results, wall = run_load(srv, sched)
+        results, wall = run_load(srv, sched, keep_solutions=False)
     srv.close()
     summ = latency_summary(results, wall)
     summ.update({"workload": "serving: resident 8^3x16, 16^3x32, 32^3x64; Poisson arrivals",

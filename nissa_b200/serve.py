@@ -237,26 +237,43 @@ def poisson_requests(n: int, rate: float, volumes, probs, seed: int = 0):
     return out
 
 
-def run_load(server: SolveServer, schedule, timeout: float = 3600.0):
-    """Submit the (time, request) schedule in real time; return the results and the wall time."""
+def _drop_solution(fut):
+    if not fut.cancelled() and fut.exception() is None:
+        fut.result().solution = None
+
+
+def run_load(server: SolveServer, schedule, timeout: float = 3600.0, keep_solutions: bool = True):
+    """Submit the (time, request) schedule in real time; return the results and the wall time.
+    With keep_solutions=False each solution is released as soon as its request
+    completes (its device memory returns to the allocator's cache for the next
+    request, as a server that hands results on would do); stats and latencies stay."""
     t0 = time.perf_counter()
     futs = []
     for t, req in schedule:
         delay = t0 + t - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        futs.append(server.submit(req))
+        fut = server.submit(req)
+        if not keep_solutions:
+            fut.add_done_callback(_drop_solution)
+        futs.append(fut)
     results = [f.result(timeout=timeout) for f in futs]
     return results, time.perf_counter() - t0
 
 
 def latency_summary(results, wall):
+    """Throughput and latency percentiles, overall and per volume; the p99 of
+    the wait for a slot (arrival to admission) and of the time in the batch
+    (admission to completion) tell queueing from solving."""
     lat = np.array([r.latency for r in results])
+    wait = np.array([r.admitted_after for r in results])
     by = collections.defaultdict(list)
     for r in results:
         by[r.request.volume].append(r.latency)
     return {"requests": len(results), "wall_s": wall, "throughput_solves_per_s": len(results) / wall,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()),
+            "admission_wait_p99_s": float(np.percentile(wait, 99)),
+            "in_batch_p99_s": float(np.percentile(lat - wait, 99)),
             "per_volume": {v: {"n": len(x), "p50_s": float(np.percentile(x, 50)), "p99_s": float(np.percentile(x, 99))}
                            for v, x in by.items()}}

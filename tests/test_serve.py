@@ -118,3 +118,17 @@ def test_poisson_schedule_and_summary():
     srv.close()
     s = latency_summary(results, wall)
     assert s["requests"] == 40 and s["p99_s"] >= s["p50_s"] > 0
+    assert s["admission_wait_p99_s"] >= 0 and s["in_batch_p99_s"] > 0
+
+
+def test_run_load_can_release_solutions():
+    """keep_solutions=False drops each solution when its request completes
+    (its memory goes back to the allocator); the stats and latencies stay."""
+    sched = poisson_requests(12, rate=1000.0, volumes=["a", "b"], probs=[0.5, 0.5], seed=5)
+    for _, r in sched:
+        r.residue = 1
+    srv = SolveServer({v: (FakeSession(4, []), make_source, 0) for v in "ab"})
+    results, wall = run_load(srv, sched, keep_solutions=False)
+    srv.close()
+    assert len(results) == 12
+    assert all(r.solution is None and r.stats["status"] == 0 and r.latency >= 0 for r in results)
