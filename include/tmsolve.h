@@ -12,7 +12,10 @@
  * fastest; e/o: lx order within each parity).  By default the pointers are
  * host pointers (copied in and out on every call); after
  * tms_set_pointer_mode(ctx, TMS_PTR_DEVICE) they are device pointers to the
- * same layout.  Every function returns a tms_status; none throws.
+ * same layout.  The library works on its own non-blocking stream: device
+ * inputs must be complete when a call is made (the caller synchronises the
+ * stream that wrote them), and every call that writes outputs has finished
+ * them when it returns.  Every function returns a tms_status; none throws.
  *
  * Residues are SQUARED relative residues, |r|^2/|b|^2, as in the reference
  * (inverters/templates/cg_invert_template_threaded.hpp:129).

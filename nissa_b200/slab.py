@@ -52,10 +52,11 @@ class Slab:
             raise TmError(st, "tms_create_slab(T=%d, t0=%d, T_loc=%d)" % (T, t0, T_loc))
         self.h = h
         self.face = int(self.lib.tms_slab_face_sites(self.h))
-        # the generic checks of a context
+        # the generic checks of a context, through a view that borrows the handle
+        # (only this object destroys it)
         self._lat = Lattice.__new__(Lattice)
-        self._lat.lib, self._lat.h = self.lib, self.h
-        self._lat.V, self._lat.Vh = self.V, self.Vh
+        self._lat.lib, self._lat.h, self._lat._owner = self.lib, self.h, False
+        self._lat.V, self._lat.Vh, self._lat.device = self.V, self.Vh, device
 
     def close(self):
         if getattr(self, "h", None):

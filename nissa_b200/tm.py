@@ -156,9 +156,10 @@ class Lattice:
         self.h = h
 
     def close(self):
-        if getattr(self, "h", None):
+        # a view that borrows another object's context (_owner False) never destroys it
+        if getattr(self, "h", None) and getattr(self, "_owner", True):
             self.lib.tms_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -180,6 +181,11 @@ class Lattice:
         if dev and any(d != dev[0] for d in dev):
             raise TypeError("mixing host and device arrays in one call")
         mode = 1 if (dev and dev[0]) else 0
+        if mode:
+            # the library reads device inputs on its own stream: the torch work
+            # that produced them (on torch's current stream) must be complete
+            import torch
+            torch.cuda.current_stream(self.device).synchronize()
         self.lib.tms_set_pointer_mode(self.h, mode)
         return mode
 

@@ -1,0 +1,123 @@
+"""Size-independent properties at the headline volume, 32^3x64 (the oracle
+finishes only small lattices in seconds, so at full size the checks are the
+operator's algebra and the solver's own FP64 residual):
+
+* device inputs written by torch are complete when the library reads them;
+* linearity of the FP64 operator Q = g5 D_tm: Q(a x + b y) = a Q x + b Q y;
+* Q(+mu)^+ = Q(-mu): <x, Q(+mu) y> = <Q(-mu) x, y>;
+* the mixed-precision full solve (FP16 inner, the headline's path) and the
+  FP32-inner one reach the target true residual, recomputed here in FP64 as
+  |source - D sol| through apply_tmQ (D = g5 Q), and agree with the FP64 solve;
+* the staged row-tile hop (launch shape 7) at every site tiling gives the
+  solution of the default shape.
+"""
+import numpy as np
+import pytest
+
+from nissa_b200 import Lattice
+from nissa_b200 import tune
+from nissa_b200 import workload as wl
+
+pytestmark = pytest.mark.gpu
+
+T, L = 64, 32
+KAPPA, MU, RES = 0.1610, 0.005, 1e-20
+
+
+@pytest.fixture(scope="module")
+def lat(cuda_device):
+    conf = wl.gauge_conf(T, L, 0.35, 1, device="cuda:0")
+    lattice = Lattice(T, L, bc_t=-1.0)
+    lattice.upload_conf(conf)
+    del conf
+    yield lattice
+    lattice.close()
+
+
+def _rand(seed):
+    import torch
+    g = torch.Generator(device="cuda:0")
+    g.manual_seed(seed)
+    return torch.randn((T * L ** 3, 4, 3, 2), dtype=torch.float64, device="cuda:0", generator=g)
+
+
+def _dot(a, b):
+    """<a, b> of two lx spinors (complex, conjugating a)."""
+    import torch
+    ca = torch.view_as_complex(a.reshape(-1, 2))
+    cb = torch.view_as_complex(b.reshape(-1, 2))
+    return complex(torch.sum(ca.conj() * cb).item())
+
+
+def _gamma5(x):
+    """g5 in the reference's chiral basis: diag(1, 1, -1, -1) over spin."""
+    y = x.clone()
+    y[:, 2:] *= -1.0
+    return y
+
+
+def test_device_inputs_ordered_after_torch(lat):
+    """A device input still being written by torch kernels when the call is
+    made is read complete (the binding waits for torch's stream): the result
+    equals the host-pointer call on the same values."""
+    import torch
+    y = _rand(5)
+    for _ in range(30):
+        y = y * 1.0000001 + 0.0
+    dev = lat.apply_tmQ(KAPPA, MU, y)
+    host = lat.apply_tmQ(KAPPA, MU, y.cpu().numpy())
+    assert float(np.linalg.norm(dev.cpu().numpy() - host) / np.linalg.norm(host)) < 1e-15
+
+
+def test_operator_linearity(lat):
+    import torch
+    x, y = _rand(1), _rand(2)
+    a, b = 0.37, -1.25
+    lhs = lat.apply_tmQ(KAPPA, MU, a * x + b * y)
+    rhs = a * lat.apply_tmQ(KAPPA, MU, x) + b * lat.apply_tmQ(KAPPA, MU, y)
+    assert float(torch.linalg.norm(lhs - rhs) / torch.linalg.norm(rhs)) < 1e-14
+
+
+def test_operator_adjoint(lat):
+    import torch
+    x, y = _rand(3), _rand(4)
+    qy = lat.apply_tmQ(KAPPA, MU, y)
+    left = _dot(x, qy)
+    right = _dot(lat.apply_tmQ(KAPPA, -MU, x), y)
+    scale = float(torch.linalg.norm(x) * torch.linalg.norm(qy))
+    assert abs(left - right) / scale < 1e-14
+
+
+@pytest.mark.parametrize("precision", ["half", "single"])
+def test_mixed_solve_true_residual(lat, precision):
+    import torch
+    src = torch.zeros((T * L ** 3, 4, 3, 2), dtype=torch.float64, device="cuda:0")
+    src[0, 1, 2, 0] = 1.0
+    ref, st64 = lat.inv_tmD_cg_eoprec(KAPPA, MU, src, 100000, RES, precision="double")
+    sol, st = lat.inv_tmD_cg_eoprec(KAPPA, MU, src, 100000, RES, precision=precision)
+    # D sol = g5 Q sol, recomputed in FP64 outside the solver
+    r = src - _gamma5(lat.apply_tmQ(KAPPA, MU, sol))
+    res2 = float(torch.sum(r * r) / torch.sum(src * src))
+    assert res2 < 10 * RES, res2
+    assert st["true_rel_res2"] < RES
+    assert float(torch.linalg.norm(sol - ref) / torch.linalg.norm(ref)) < 1e-9
+    assert abs(st["iterations"] - st64["iterations"]) <= 0.1 * st64["iterations"] + 2
+
+
+def test_staged_tilings_agree(lat):
+    import torch
+    src = torch.zeros((T * L ** 3, 4, 3, 2), dtype=torch.float64, device="cuda:0")
+    src[0, 0, 0, 0] = 1.0
+    base, _ = lat.inv_tmD_cg_eoprec(KAPPA, MU, src, 100000, RES, precision="half")
+    shape0 = lat.get_tuning("hop_cfg_half")
+    try:
+        lat.set_tuning("hop_cfg_half", tune.TILED_SHAPE)
+        for rows in tune.tile_rows_choices(L, L):
+            lat.set_tuning("tma_rows", rows)
+            sol, st = lat.inv_tmD_cg_eoprec(KAPPA, MU, src, 100000, RES, precision="half")
+            assert st["true_rel_res2"] < RES, rows
+            assert float(torch.linalg.norm(sol - base) / torch.linalg.norm(base)) < 1e-9, rows
+        assert lat.hop_stage_timeouts == 0
+    finally:
+        lat.set_tuning("hop_cfg_half", shape0)
+        lat.set_tuning("tma_rows", 0)
