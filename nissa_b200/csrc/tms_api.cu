@@ -236,7 +236,7 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
   if (!ctx->U64) CU(cudaMalloc(&ctx->U64, (size_t)V * 36 * sizeof(double2)));
   if (!ctx->U32r) CU(cudaMalloc(&ctx->U32r, (size_t)V * 12 * sizeof(float4)));
   if (!ctx->U32f) CU(cudaMalloc(&ctx->U32f, (size_t)V * 36 * sizeof(float2)));
-  if (!ctx->U16r) CU(cudaMalloc(&ctx->U16r, 8 * LinkT<LINK_I16_12>::block_bytes(ctx->g.Vh)));
+  if (!ctx->U16r) CU(cudaMalloc(&ctx->U16r, LinkT<LINK_I16_12>::bytes(ctx->g.Vh)));
   const double* src = conf;
   if (ctx->ptr_mode == TMS_PTR_HOST)
     {

@@ -438,16 +438,15 @@ namespace tms_int
         Ur[((size_t)pm * 3 + 2) * Vh + site] = make_float4((float)u[4].re, (float)u[4].im, (float)u[5].re, (float)u[5].im);
         auto q = [](double x) { return (short)__double2int_rn(fmin(1.0, fmax(-1.0, x)) * 32767.0); };
         {
-          // the LinkT<LINK_I16_12> block of (par, mu): shorts 0-7 as a 16-byte word, 8-11 as an 8-byte word
+          // LinkT<LINK_I16_12>: shorts 0-7 as a 16-byte word, 8-11 as an 8-byte word
           const short4 a0 = make_short4(q(u[0].re), q(u[0].im), q(u[1].re), q(u[1].im));
           const short4 a1 = make_short4(q(u[2].re), q(u[2].im), q(u[3].re), q(u[3].im));
           const short4 a2 = make_short4(q(u[4].re), q(u[4].im), q(u[5].re), q(u[5].im));
-          char* blk = Us + (size_t)pm * LinkT<LINK_I16_12>::block_bytes(Vh);
           uint4 w;
           memcpy(&w.x, &a0, 8);
           memcpy(&w.z, &a1, 8);
-          reinterpret_cast<uint4*>(blk)[site] = w;
-          reinterpret_cast<short4*>(blk + (size_t)16 * Vh)[site] = a2;
+          reinterpret_cast<uint4*>(Us)[(size_t)pm * Vh + site] = w;
+          reinterpret_cast<short4*>(Us + (size_t)128 * Vh)[(size_t)pm * Vh + site] = a2;
         }
         // deviation of row 2 from conj(row0 x row1), plus row-0/1 unitarity
         const C<double> c0 = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
