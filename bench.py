@@ -457,7 +457,10 @@ def headline_tuning(lat, args):
         lat.set_tuning("hop_cfg_" + prec, args.hop_cfg)
         if args.tma_rows >= 0:
             lat.set_tuning("tma_rows", args.tma_rows)
-        return {"source": "command line", "settings": {"hop_cfg_" + prec: args.hop_cfg, "tma_rows": args.tma_rows}}
+        settings = {"hop_cfg_" + prec: args.hop_cfg}
+        if args.tma_rows >= 0:
+            settings["tma_rows"] = args.tma_rows
+        return {"source": "command line", "settings": settings}
     from nissa_b200 import tune
     t0 = time.perf_counter()
     r = tune.autotune(lat, prec)
