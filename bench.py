@@ -344,16 +344,27 @@ def run_ours(args):
 
     # --- the other inner precisions on the same solves (solver-reported device seconds) -----
     variants = {}
-    for name, vp, links16 in (("single_links32", "single", 0), ("single", "single", 1), ("half", "half", 1)):
-        if vp == prec and (links16 or vp == "half"):
+    for name, vp, links16 in (("single_links32", "single", 0), ("single", "single", 1), ("half", "half", 1),
+                              ("half_fp16_arithmetic", "half", 1)):
+        if vp == prec and (links16 or vp == "half") and name != "half_fp16_arithmetic":
             continue
         lat.set_tuning("links_single", links16)
+        lat.set_tuning("half_arith", 1 if name == "half_fp16_arithmetic" else 0)
         solve(0, precision=vp)
         vs = [solve(k, precision=vp) for k in range(2)]
         variants[name] = {"solves_per_s": 1.0 / statistics.mean(x["seconds"] for x in vs),
                           "iterations": vs[0]["iterations"], "reliable_updates": vs[0]["reliable_updates"],
                           "true_rel_res2_max": max(x["true_rel_res2"] for x in vs)}
+        if name == "half_fp16_arithmetic":
+            # against the FP32-arithmetic FP16 solver timed the same way, and column 0 against FP64
+            solve(0, out=sol)
+            variants[name]["rel_err_vs_fp64"] = float(torch.linalg.norm(sol - ref) / torch.linalg.norm(ref))
+            lat.set_tuning("half_arith", 0)
+            base = [solve(k, precision=vp) for k in range(2)]
+            variants[name]["speedup_vs_fp32_arithmetic"] = (statistics.mean(x["seconds"] for x in base) /
+                                                            statistics.mean(x["seconds"] for x in vs))
     lat.set_tuning("links_single", 1)
+    lat.set_tuning("half_arith", 0)
 
     # --- CPU baseline: one whole reference solve of column 0 (rank 0, N=1 only), and the -------
     # --- headline solution's error against it -------------------------------------------------

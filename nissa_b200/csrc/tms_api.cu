@@ -173,6 +173,7 @@ tms_status tms_destroy(tms_ctx* ctx)
   fr(ctx->U32r);
   fr(ctx->U32f);
   fr(ctx->U16r);
+  fr(ctx->U16h);
   fr(ctx->prm);
   fr(ctx->st);
   fr(ctx->red_partial);
@@ -237,6 +238,7 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
   if (!ctx->U32r) CU(cudaMalloc(&ctx->U32r, (size_t)V * 12 * sizeof(float4)));
   if (!ctx->U32f) CU(cudaMalloc(&ctx->U32f, (size_t)V * 36 * sizeof(float2)));
   if (!ctx->U16r) CU(cudaMalloc(&ctx->U16r, LinkT<LINK_I16_12>::bytes(ctx->g.Vh)));
+  if (!ctx->U16h) CU(cudaMalloc(&ctx->U16h, LinkT<LINK_H16_12>::bytes(ctx->g.Vh)));
   const double* src = conf;
   if (ctx->ptr_mode == TMS_PTR_HOST)
     {
@@ -250,7 +252,7 @@ tms_status tms_conf_upload(tms_ctx* ctx, const double* conf, int layout, int fla
   CU(cudaGetLastError());
   const int64_t nl = 8 * Vh;
   ++ctx->launches;
-  conf_lowprec_kernel<<<div_up(nl, 256), 256, 0, ctx->stream>>>(nl, (int)Vh, ctx->U64, ctx->U32r, ctx->U32f, ctx->U16r,
+  conf_lowprec_kernel<<<div_up(nl, 256), 256, 0, ctx->stream>>>(nl, (int)Vh, ctx->U64, ctx->U32r, ctx->U32f, ctx->U16r, ctx->U16h,
                                                                  reducer(ctx));
   CU(cudaGetLastError());
   const double dev = read_result(ctx);
@@ -437,6 +439,13 @@ tms_status tms_set_tuning(tms_ctx* ctx, const char* key, double value)
       ctx->hop_cfg[p] = v;
       return TMS_OK;
     }
+  if (k == "half_arith")
+    {
+      if (value != 0.0 && value != 1.0) return fail(ctx, TMS_ERR_BAD_ARG, "half_arith: 0 (FP32 arithmetic) or 1");
+      if (ctx->half_arith != (int)value) drop_all();
+      ctx->half_arith = (int)value;
+      return TMS_OK;
+    }
   if (k == "tma_rows")
     {
       const int v = (int)value;
@@ -542,6 +551,7 @@ tms_status tms_get_tuning(tms_ctx* ctx, const char* key, double* value)
   else if (k == "hop_cfg_single") *value = ctx->hop_cfg[PREC_F32];
   else if (k == "hop_cfg_half") *value = ctx->hop_cfg[PREC_F16];
   else if (k == "tma_rows") *value = ctx->tma_rows;
+  else if (k == "half_arith") *value = ctx->half_arith;
   else if (k == "graph_iters") *value = ctx->graph_iters;
   else if (k == "batch_graph_iters") *value = ctx->batch_iters;
   else if (k == "mrhs_per_thread") *value = ctx->mrhs_r;

@@ -3,6 +3,7 @@
 // full-lattice CG of Q(+m)Q(-m) and the multi-shift CGM of the tm Q^2
 // operator.  Each CG/CGM iteration block is replayed as a CUDA graph.
 #include "tms_internal.cuh"
+#include <type_traits>
 
 #include <algorithm>
 
@@ -537,8 +538,14 @@ namespace
                                    : cg_mixed<Op, PREC_F32>(ctx, links32r(ctx), niter, residue, have_guess, stats);
       }
     if (precision == TMS_PREC_MIXED_HALF)
-      return ctx->su3 ? cg_mixed<Op, PREC_F16>(ctx, links16r(ctx), niter, residue, have_guess, stats)
-                      : cg_mixed<Op, PREC_F16>(ctx, links32f(ctx), niter, residue, have_guess, stats);
+      {
+        // the e/o twisted-mass solver may run its hops in FP16 arithmetic (tuning "half_arith")
+        if constexpr (std::is_same<Op, EoOp>::value)
+          if (ctx->su3 && ctx->half_arith)
+            return cg_mixed<Op, PREC_F16>(ctx, links16h(ctx), niter, residue, have_guess, stats);
+        return ctx->su3 ? cg_mixed<Op, PREC_F16>(ctx, links16r(ctx), niter, residue, have_guess, stats)
+                        : cg_mixed<Op, PREC_F16>(ctx, links32f(ctx), niter, residue, have_guess, stats);
+      }
     return fail(ctx, TMS_ERR_BAD_ARG, "unknown precision %d", precision);
   }
 

@@ -18,6 +18,7 @@
 //                                                   the first 8 of the 12 shorts in one 16-byte
 //                                                   word (copied past L1, no reuse), the last 4 in
 //                                                   one 8-byte word
+//   links,  H16    as I16, the 12 reals as FP16 values (FP16-arithmetic hop only)
 //
 // Sites of one parity are numbered as the reference numbers them
 // (geometry_eo.cpp:66-77): lx = ((t*LX + x)*LY + y)*LZ + z, and the e/o index
@@ -32,7 +33,7 @@
 namespace tms
 {
   enum Prec { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2 };
-  enum LinkFmt { LINK_F64_18 = 0, LINK_F32_12 = 1, LINK_F32_18 = 2, LINK_I16_12 = 3, LINK_F64_12 = 4 };
+  enum LinkFmt { LINK_F64_18 = 0, LINK_F32_12 = 1, LINK_F32_18 = 2, LINK_I16_12 = 3, LINK_F64_12 = 4, LINK_H16_12 = 5 };
 
   // ------------------------------------------------------------- geometry
   struct Lattice
@@ -472,6 +473,25 @@ namespace tms
       u[6] = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));
       u[7] = cconj(csub(cmul(u[2], u[3]), cmul(u[0], u[5])));
       u[8] = cconj(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));
+    }
+  };
+
+  // The 12 reals of rows 0 and 1 as FP16 values (not fixed point), in the same
+  // two arrays of planes as LinkT<LINK_I16_12>: read only by the pipelined FP16
+  // hop with FP16 arithmetic (tuning "half_arith"), which rebuilds row 2 in FP16
+  template <> struct LinkT<LINK_H16_12>
+  {
+    using R = float;
+    const char* __restrict__ d;
+    int Vh;
+    __host__ __device__ static size_t bytes(int64_t Vh) { return (size_t)192 * Vh; }
+    __device__ __forceinline__ const uint4* w16(int par, int mu) const
+    {
+      return reinterpret_cast<const uint4*>(d) + (size_t)(par * 4 + mu) * Vh;
+    }
+    __device__ __forceinline__ const uint2* w8(int par, int mu) const
+    {
+      return reinterpret_cast<const uint2*>(d + (size_t)128 * Vh) + (size_t)(par * 4 + mu) * Vh;
     }
   };
 

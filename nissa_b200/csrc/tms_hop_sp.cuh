@@ -247,8 +247,8 @@ namespace tms
   {
     static constexpr int KS = (P == PREC_F16) ? 3 : 6;                                 // spinor, 16-byte words
     static constexpr int HASN = (P == PREC_F16) ? 1 : 0;                               // FP16 per-site factor
-    static constexpr int KL16 = (LF == LINK_F32_12) ? 3 : (LF == LINK_I16_12) ? 1 : 0;    // link, 16-byte words
-    static constexpr int KL8 = (LF == LINK_I16_12) ? 1 : (LF == LINK_F32_18) ? 9 : 0;     // link, 8-byte words
+    static constexpr int KL16 = (LF == LINK_F32_12) ? 3 : (LF == LINK_I16_12 || LF == LINK_H16_12) ? 1 : 0; // link, 16-byte words
+    static constexpr int KL8 = (LF == LINK_I16_12 || LF == LINK_H16_12) ? 1 : (LF == LINK_F32_18) ? 9 : 0;  // link, 8-byte words
     static constexpr int W16 = KS + KL16;
     static constexpr int SLOT_BYTES = W16 * 16 + KL8 * 8 + HASN * 4;
     template <int DIST>
@@ -289,7 +289,7 @@ namespace tms
 #pragma unroll
     for (int k = 0; k < F::KS; k++) cp_async16(sl.w16(slot, k), sp + (size_t)k * in.stride + n);
     if (F::HASN) cp_async4(sl.nrm(slot), in.n + n);
-    if constexpr (LF == LINK_I16_12)
+    if constexpr (LF == LINK_I16_12 || LF == LINK_H16_12)
       {
         // the 16-byte word past L1 (a link is read once), the 8-byte word through it
         cp_async16_stream(sl.w16(slot, F::KS), U.w16(lpar, MU) + ls);
@@ -378,17 +378,161 @@ namespace tms
       }
   }
 
+  // One direction in FP16 arithmetic (the FP16-arithmetic hop, links LINK_H16_12):
+  // the neighbour's stored half2 words w[12] ((re, im) of component spin*3 +
+  // colour, in stored units) are projected in half2 arithmetic with the two
+  // spin rows in the lanes, row 2 of the link is rebuilt from the FP16 rows 0
+  // and 1 (complex multiply-adds on (re, im) half2), the SU(3) product runs in
+  // half2 fused multiply-adds with each link element broadcast to both lanes,
+  // and the result is widened to FP32 pairs and accumulated times f as in
+  // sp_dir_compute.  FP16 products and sums add a rounding of 2^-11 relative to
+  // the FP16 storage of the spinors (5.9e-4 from the FP32-arithmetic hop on
+  // random fields at 32^3x64).
+  template <int MU, bool FWD>
+  __device__ __forceinline__ void hp_dir_compute(const unsigned w[12], const __half2 lr[6], float f, C<P2> A01[3],
+                                                 C<P2> A23[3])
+  {
+    constexpr bool CROSS = (MU == 1 || MU == 2);
+    const __half2 pm = __floats2half2_rn(1.f, -1.f), mp = __floats2half2_rn(-1.f, 1.f);
+    __half2 Hre[3], Him[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      {
+        const __half2 s0 = *reinterpret_cast<const __half2*>(&w[c]), s1 = *reinterpret_cast<const __half2*>(&w[3 + c]);
+        const __half2 s2 = *reinterpret_cast<const __half2*>(&w[6 + c]), s3 = *reinterpret_cast<const __half2*>(&w[9 + c]);
+        const __half2 are = __lows2half2(s0, s1), aim = __highs2half2(s0, s1);
+        const __half2 bre = CROSS ? __lows2half2(s3, s2) : __lows2half2(s2, s3);
+        const __half2 bim = CROSS ? __highs2half2(s3, s2) : __highs2half2(s2, s3);
+        if (MU == 0)
+          {
+            Hre[c] = FWD ? __hadd2(are, bre) : __hsub2(are, bre);
+            Him[c] = FWD ? __hadd2(aim, bim) : __hsub2(aim, bim);
+          }
+        if (MU == 1)
+          {
+            Hre[c] = FWD ? __hsub2(are, bim) : __hadd2(are, bim);
+            Him[c] = FWD ? __hadd2(aim, bre) : __hsub2(aim, bre);
+          }
+        if (MU == 2)
+          {
+            Hre[c] = __hfma2(FWD ? pm : mp, bre, are);
+            Him[c] = __hfma2(FWD ? pm : mp, bim, aim);
+          }
+        if (MU == 3)
+          {
+            Hre[c] = __hfma2(FWD ? mp : pm, bim, are);
+            Him[c] = __hfma2(FWD ? pm : mp, bre, aim);
+          }
+      }
+    // row 2 = conj(row0 x row1)
+    const __half2 cj = __floats2half2_rn(1.f, -1.f), zero = __float2half2_rn(0.f);
+    __half2 L[9];
+#pragma unroll
+    for (int k = 0; k < 6; k++) L[k] = lr[k];
+    L[6] = __hmul2(cj, __hcmadd(lr[1], lr[5], __hneg2(__hcmadd(lr[2], lr[4], zero))));
+    L[7] = __hmul2(cj, __hcmadd(lr[2], lr[3], __hneg2(__hcmadd(lr[0], lr[5], zero))));
+    L[8] = __hmul2(cj, __hcmadd(lr[0], lr[4], __hneg2(__hcmadd(lr[1], lr[3], zero))));
+    // forward: re += er hr - ei hi, im += er hi + ei hr; backward (U^+): re += er hr + ei hi, im += er hi - ei hr
+    C<P2> u[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+      {
+        __half2 ure, uim;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+          {
+            const __half2 e = FWD ? L[3 * i + j] : L[3 * j + i];
+            const __half2 er = __low2half2(e), ei = __high2half2(e);
+            if (j == 0)
+              {
+                ure = __hmul2(er, Hre[j]);
+                uim = __hmul2(er, Him[j]);
+              }
+            else
+              {
+                ure = __hfma2(er, Hre[j], ure);
+                uim = __hfma2(er, Him[j], uim);
+              }
+            ure = __hfma2(FWD ? __hneg2(ei) : ei, Him[j], ure);
+            uim = __hfma2(FWD ? ei : __hneg2(ei), Hre[j], uim);
+          }
+        u[i].re = P2{__half22float2(ure)};
+        u[i].im = P2{__half22float2(uim)};
+      }
+    const P2 F = bcast(f), NF = bcast(-f), Fpm = p2(f, -f), Fmp = p2(-f, f);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      {
+        A01[c].re = fma2(F, u[c].re, A01[c].re);
+        A01[c].im = fma2(F, u[c].im, A01[c].im);
+        C<P2>& A = A23[c];
+        const C<P2> v = u[c];
+        if (MU == 0)
+          {
+            A.re = fma2(FWD ? F : NF, v.re, A.re);
+            A.im = fma2(FWD ? F : NF, v.im, A.im);
+          }
+        if (MU == 3)
+          {
+            A.re = fma2(FWD ? Fpm : Fmp, v.im, A.re);
+            A.im = fma2(FWD ? Fmp : Fpm, v.re, A.im);
+          }
+        if (MU == 1)
+          {
+            const float sg = FWD ? f : -f;
+            A.re.v.x = fmaf(sg, v.im.v.y, A.re.v.x);
+            A.im.v.x = fmaf(-sg, v.re.v.y, A.im.v.x);
+            A.re.v.y = fmaf(sg, v.im.v.x, A.re.v.y);
+            A.im.v.y = fmaf(-sg, v.re.v.x, A.im.v.y);
+          }
+        if (MU == 2)
+          {
+            const float sg = FWD ? f : -f;
+            A.re.v.x = fmaf(-sg, v.re.v.y, A.re.v.x);
+            A.im.v.x = fmaf(-sg, v.im.v.y, A.im.v.x);
+            A.re.v.y = fmaf(sg, v.re.v.x, A.re.v.y);
+            A.im.v.y = fmaf(sg, v.im.v.x, A.im.v.y);
+          }
+      }
+  }
+
   template <int D, int P, int LF, int SLOTS>
   __device__ __forceinline__ void spp_compute(const SppSlots<P, LF, SLOTS>& sl, const Lattice& g, bool w, float anis,
                                               C<P2> A01[3], C<P2> A23[3])
   {
     constexpr int MU = D / 2;
-    C<float> sp[12], L[9];
-    float ss, ls;
-    spp_read<P, LF, SLOTS>(sl, D % SLOTS, sp, ss, L, ls);
     const float fmu = MU ? anis : 1.0f;
-    const float f = (w ? fmu * float(g.bc_t) : fmu) * ss * ls;
-    sp_dir_compute<MU, (D % 2) == 0, LF == LINK_I16_12>(sp, L, f, A01, A23, 1.0f / 32767.0f);
+    if constexpr (LF == LINK_H16_12)
+      {
+        // FP16 spinor words and FP16 link rows straight from the slot
+        const int slot = D % SLOTS;
+        unsigned sw[12];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+          {
+            const uint4 x = *sl.w16(slot, k);
+            sw[4 * k] = x.x;
+            sw[4 * k + 1] = x.y;
+            sw[4 * k + 2] = x.z;
+            sw[4 * k + 3] = x.w;
+          }
+        const uint4 a = *sl.w16(slot, SppFmt<P, LF>::KS);
+        const uint2 b = *sl.w8(slot, 0);
+        const unsigned lw[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+        __half2 lr[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) lr[k] = *reinterpret_cast<const __half2*>(&lw[k]);
+        const float f = (w ? fmu * float(g.bc_t) : fmu) * *sl.nrm(slot);
+        hp_dir_compute<MU, (D % 2) == 0>(sw, lr, f, A01, A23);
+      }
+    else
+      {
+        C<float> sp[12], L[9];
+        float ss, ls;
+        spp_read<P, LF, SLOTS>(sl, D % SLOTS, sp, ss, L, ls);
+        const float f = (w ? fmu * float(g.bc_t) : fmu) * ss * ls;
+        sp_dir_compute<MU, (D % 2) == 0, LF == LINK_I16_12>(sp, L, f, A01, A23, 1.0f / 32767.0f);
+      }
   }
 
   // an FP16 field at site `site` into a slot's spinor words (an epilogue operand)

@@ -63,6 +63,7 @@ struct tms_ctx
   float4* U32r = nullptr; // 12-real
   float2* U32f = nullptr; // 18-real
   char* U16r = nullptr; // 12-real, 16-bit fixed point (LinkT<LINK_I16_12> blocks)
+  char* U16h = nullptr; // 12-real, FP16 values (LinkT<LINK_H16_12>), for the FP16-arithmetic hop
 
   // scalars and reduction scratch
   OpParams* prm = nullptr;       // [2]: operator params (slot 0 solver, slot 1 free use)
@@ -142,6 +143,7 @@ struct tms_ctx
   int tma_rows = 0; // lattice rows per tile of the staged hop (launch shape 7): 0 the most that fit
   double delta_single = 1e-3, delta_half = 0.005;
   int single_links16 = 1; // FP32-spinor inner solver on 16-bit fixed-point links (1) or FP32 12-real links (0)
+  int half_arith = 0; // FP16-spinor e/o solver: FP32 arithmetic (0) or the FP16-arithmetic pipelined hop (1)
   int reliable_links12 = 1; // FP64 residuals of the mixed solvers on 12-real FP64 links (when SU(3) to rounding)
   double su3_dev = 1.0;     // largest deviation of the resident links from SU(3) (unitarity, row 2)
   int mrhs_r = 1; // right-hand sides per thread in the batched hopping kernel (1, 2, 4; FP64 at most 2)
@@ -299,81 +301,96 @@ namespace tms_int
   {
     const int nsite = (int)(npar * c->g.Vh);
     ++c->launches;
-    if constexpr (P != PREC_F64)
+    if constexpr (LF == LINK_H16_12)
       {
-        if (c->hop_cfg[P] == 5)
-          {
-            launch_pdl(c, hop_sp_kernel<P, LF, Epi, Fin>, div_up(nsite, HOP_SP_THREADS), HOP_SP_THREADS, 0, s, c->g,
-                       par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
-            return;
-          }
-        if (c->hop_cfg[P] == 6)
-          {
-            // two directions ahead: three slots of 76 B (FP16) per thread keep 5 blocks per SM
-            // with ~90 KB of L1 left for the neighbours' reuse (three ahead left ~30 KB: 4 % slower)
-            constexpr int DIST = 2;
-            constexpr int MINB = (P == PREC_F16) ? 5 : 3;
-            constexpr int smem = SppFmt<P, LF>::template smem<DIST>();
-            auto k = hop_spp_kernel<P, LF, Epi, Fin, DIST, MINB>;
-            static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            (void)attr;
-            launch_pdl(c, k, div_up(nsite, SPP_THREADS), SPP_THREADS, smem, s, c->g, par_out, npar, in_e, in_o, U, prm,
-                       epi, reducer(c), fin, stop);
-            return;
-          }
-        if constexpr (LF == LINK_I16_12 || LF == LINK_F32_12)
-          if (c->hop_cfg[P] == 7)
-            {
-              const TmaGeom G = tma_geom(c->g, c->tma_timeouts, c->tma_rows);
-              const int ntiles = G.ns ? (int)(npar * c->g.Vh / G.ns) : 0;
-              if (G.ns && ntiles <= c->red_cap)
-                {
-                  const size_t smem = tma_smem_bytes<P, LF>(G.nc, G.ns);
-                  auto k = hop_tma_kernel<P, LF, Epi, Fin>;
-                  // the largest tile: at most HOP_TMA_THREADS sites and two halo rows of at most 64 sites
-                  static const cudaError_t a1 = cudaFuncSetAttribute(
-                    k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                    (int)tma_smem_bytes<P, LF>(HOP_TMA_THREADS + 128, HOP_TMA_THREADS));
-                  static const cudaError_t a2 = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-                  (void)a1;
-                  (void)a2;
-                  launch_pdl(c, k, ntiles, HOP_TMA_THREADS, smem, s, c->g, G, par_out, npar, in_e, in_o, U, prm, epi,
-                             reducer(c), fin, stop);
-                  return;
-                }
-            }
+        // FP16 arithmetic: the pipelined one-site kernel only
+        constexpr int DIST = 2, MINB = 5;
+        constexpr int smem = SppFmt<P, LF>::template smem<DIST>();
+        auto k = hop_spp_kernel<P, LF, Epi, Fin, DIST, MINB>;
+        static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        (void)attr;
+        launch_pdl(c, k, div_up(nsite, SPP_THREADS), SPP_THREADS, smem, s, c->g, par_out, npar, in_e, in_o, U, prm, epi,
+                   reducer(c), fin, stop);
+        return;
       }
-    if constexpr (P != PREC_F64)
-      if ((c->hop_cfg[P] == 3 || c->hop_cfg[P] == 4) && c->g.T % 4 == 0)
-        {
-          const int n2 = nsite / 2;
-          if (c->hop_cfg[P] == 4)
-            launch_pdl(c, hop2_kernel<P, LF, Epi, Fin>, div_up(n2, HOP2_THREADS), HOP2_THREADS, 0, s, c->g, par_out,
-                       npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
-          else
-            {
-              constexpr int smem = PipeFmt<P, LF>::SMEM;
-              static const cudaError_t attr = cudaFuncSetAttribute(
-                hop_pipe_kernel<P, LF, Epi, Fin>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-              (void)attr;
-              launch_pdl(c, hop_pipe_kernel<P, LF, Epi, Fin>, div_up(n2, PIPE_THREADS), PIPE_THREADS, smem, s, c->g,
-                         par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
-            }
-          return;
-        }
-    switch (c->hop_cfg[P])
+    else
       {
-      case 1:
-        launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 1>, div_up(nsite, HopCfg<P, 1>::NT), HopCfg<P, 1>::NT, 0, s, c->g,
-                   par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
-        break;
-      case 2:
-        launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 2>, div_up(nsite, HopCfg<P, 2>::NT), HopCfg<P, 2>::NT, 0, s, c->g,
-                   par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
-        break;
-      default:
-        launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 0>, div_up(nsite, HopCfg<P, 0>::NT), HopCfg<P, 0>::NT, 0, s, c->g,
-                   par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+    if constexpr (P != PREC_F64)
+          {
+            if (c->hop_cfg[P] == 5)
+              {
+                launch_pdl(c, hop_sp_kernel<P, LF, Epi, Fin>, div_up(nsite, HOP_SP_THREADS), HOP_SP_THREADS, 0, s, c->g,
+                           par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+                return;
+              }
+            if (c->hop_cfg[P] == 6)
+              {
+                // two directions ahead: three slots of 76 B (FP16) per thread keep 5 blocks per SM
+                // with ~90 KB of L1 left for the neighbours' reuse (three ahead left ~30 KB: 4 % slower)
+                constexpr int DIST = 2;
+                constexpr int MINB = (P == PREC_F16) ? 5 : 3;
+                constexpr int smem = SppFmt<P, LF>::template smem<DIST>();
+                auto k = hop_spp_kernel<P, LF, Epi, Fin, DIST, MINB>;
+                static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                (void)attr;
+                launch_pdl(c, k, div_up(nsite, SPP_THREADS), SPP_THREADS, smem, s, c->g, par_out, npar, in_e, in_o, U, prm,
+                           epi, reducer(c), fin, stop);
+                return;
+              }
+            if constexpr (LF == LINK_I16_12 || LF == LINK_F32_12)
+              if (c->hop_cfg[P] == 7)
+                {
+                  const TmaGeom G = tma_geom(c->g, c->tma_timeouts, c->tma_rows);
+                  const int ntiles = G.ns ? (int)(npar * c->g.Vh / G.ns) : 0;
+                  if (G.ns && ntiles <= c->red_cap)
+                    {
+                      const size_t smem = tma_smem_bytes<P, LF>(G.nc, G.ns);
+                      auto k = hop_tma_kernel<P, LF, Epi, Fin>;
+                      // the largest tile: at most HOP_TMA_THREADS sites and two halo rows of at most 64 sites
+                      static const cudaError_t a1 = cudaFuncSetAttribute(
+                        k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                        (int)tma_smem_bytes<P, LF>(HOP_TMA_THREADS + 128, HOP_TMA_THREADS));
+                      static const cudaError_t a2 = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                      (void)a1;
+                      (void)a2;
+                      launch_pdl(c, k, ntiles, HOP_TMA_THREADS, smem, s, c->g, G, par_out, npar, in_e, in_o, U, prm, epi,
+                                 reducer(c), fin, stop);
+                      return;
+                    }
+                }
+          }
+        if constexpr (P != PREC_F64)
+          if ((c->hop_cfg[P] == 3 || c->hop_cfg[P] == 4) && c->g.T % 4 == 0)
+            {
+              const int n2 = nsite / 2;
+              if (c->hop_cfg[P] == 4)
+                launch_pdl(c, hop2_kernel<P, LF, Epi, Fin>, div_up(n2, HOP2_THREADS), HOP2_THREADS, 0, s, c->g, par_out,
+                           npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+              else
+                {
+                  constexpr int smem = PipeFmt<P, LF>::SMEM;
+                  static const cudaError_t attr = cudaFuncSetAttribute(
+                    hop_pipe_kernel<P, LF, Epi, Fin>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                  (void)attr;
+                  launch_pdl(c, hop_pipe_kernel<P, LF, Epi, Fin>, div_up(n2, PIPE_THREADS), PIPE_THREADS, smem, s, c->g,
+                             par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+                }
+              return;
+            }
+        switch (c->hop_cfg[P])
+          {
+          case 1:
+            launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 1>, div_up(nsite, HopCfg<P, 1>::NT), HopCfg<P, 1>::NT, 0, s, c->g,
+                       par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+            break;
+          case 2:
+            launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 2>, div_up(nsite, HopCfg<P, 2>::NT), HopCfg<P, 2>::NT, 0, s, c->g,
+                       par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+            break;
+          default:
+            launch_pdl(c, hop_kernel<P, LF, Epi, Fin, 0>, div_up(nsite, HopCfg<P, 0>::NT), HopCfg<P, 0>::NT, 0, s, c->g,
+                       par_out, npar, in_e, in_o, U, prm, epi, reducer(c), fin, stop);
+          }
       }
   }
 
@@ -393,6 +410,7 @@ namespace tms_int
   inline LinkT<LINK_F32_12> links32r(tms_ctx* c) { return LinkT<LINK_F32_12>{c->U32r, (int)c->g.Vh}; }
   inline LinkT<LINK_F32_18> links32f(tms_ctx* c) { return LinkT<LINK_F32_18>{c->U32f, (int)c->g.Vh}; }
   inline LinkT<LINK_I16_12> links16r(tms_ctx* c) { return LinkT<LINK_I16_12>{c->U16r, (int)c->g.Vh}; }
+  inline LinkT<LINK_H16_12> links16h(tms_ctx* c) { return LinkT<LINK_H16_12>{c->U16h, (int)c->g.Vh}; }
 
   // --------------------------------------------------------- conf kernels
   static __global__ void conf_to_soa_kernel(Lattice g, const double* __restrict__ src, int layout, int unfold,
@@ -419,6 +437,7 @@ namespace tms_int
   // FP32 copies and the special-unitarity check (max deviation over links)
   static __global__ void conf_lowprec_kernel(int64_t nlinks_per_parmu, int Vh, const double2* __restrict__ U,
                                       float4* __restrict__ Ur, float2* __restrict__ Uf, char* __restrict__ Us,
+                                      char* __restrict__ Uh,
                                       Reducer red)
   {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; // over 8*Vh (par,mu,site)
@@ -447,6 +466,16 @@ namespace tms_int
           memcpy(&w.z, &a1, 8);
           reinterpret_cast<uint4*>(Us)[(size_t)pm * Vh + site] = w;
           reinterpret_cast<short4*>(Us + (size_t)128 * Vh)[(size_t)pm * Vh + site] = a2;
+          // LinkT<LINK_H16_12>: the same 12 reals as FP16 values, same planes
+          __half2 hv[6];
+#pragma unroll
+          for (int k = 0; k < 6; k++) hv[k] = __floats2half2_rn((float)u[k].re, (float)u[k].im);
+          uint4 wh;
+          uint2 wh2;
+          memcpy(&wh, hv, 16);
+          memcpy(&wh2, hv + 4, 8);
+          reinterpret_cast<uint4*>(Uh)[(size_t)pm * Vh + site] = wh;
+          reinterpret_cast<uint2*>(Uh + (size_t)128 * Vh)[(size_t)pm * Vh + site] = wh2;
         }
         // deviation of row 2 from conj(row0 x row1), plus row-0/1 unitarity
         const C<double> c0 = cconj(csub(cmul(u[1], u[5]), cmul(u[2], u[4])));

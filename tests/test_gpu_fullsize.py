@@ -5,8 +5,8 @@ operator's algebra and the solver's own FP64 residual):
 * device inputs written by torch are complete when the library reads them;
 * linearity of the FP64 operator Q = g5 D_tm: Q(a x + b y) = a Q x + b Q y;
 * Q(+mu)^+ = Q(-mu): <x, Q(+mu) y> = <Q(-mu) x, y>;
-* the mixed-precision full solve (FP16 inner, the headline's path) and the
-  FP32-inner one reach the target true residual, recomputed here in FP64 as
+* the mixed-precision full solve (FP16 inner, the headline's path; also with
+  its hops in FP16 arithmetic) and the FP32-inner one reach the target true residual, recomputed here in FP64 as
   |source - D sol| through apply_tmQ (D = g5 Q), and agree with the FP64 solve;
 * the staged row-tile hop (launch shape 7) at every site tiling gives the
   solution of the default shape.
@@ -88,9 +88,12 @@ def test_operator_adjoint(lat):
     assert abs(left - right) / scale < 1e-14
 
 
-@pytest.mark.parametrize("precision", ["half", "single"])
+@pytest.mark.parametrize("precision", ["half", "single", "half_arith"])
 def test_mixed_solve_true_residual(lat, precision):
     import torch
+    arith = precision == "half_arith"
+    precision = "half" if arith else precision
+    lat.set_tuning("half_arith", 1 if arith else 0)
     src = torch.zeros((T * L ** 3, 4, 3, 2), dtype=torch.float64, device="cuda:0")
     src[0, 1, 2, 0] = 1.0
     ref, st64 = lat.inv_tmD_cg_eoprec(KAPPA, MU, src, 100000, RES, precision="double")
@@ -102,6 +105,7 @@ def test_mixed_solve_true_residual(lat, precision):
     assert st["true_rel_res2"] < RES
     assert float(torch.linalg.norm(sol - ref) / torch.linalg.norm(ref)) < 1e-9
     assert abs(st["iterations"] - st64["iterations"]) <= 0.1 * st64["iterations"] + 2
+    lat.set_tuning("half_arith", 0)
 
 
 def test_staged_tilings_agree(lat):

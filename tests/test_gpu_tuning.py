@@ -72,6 +72,29 @@ def test_tile_rows_agree(cuda_device, T, L, precision):
                 lat.set_tuning("tma_rows", bad)
 
 
+@pytest.mark.parametrize("T,L", [(16, 8), (8, 4), (6, 4)])
+def test_half_arith_solves(cuda_device, T, L):
+    """The FP16-arithmetic hop (tuning half_arith) under the FP16-spinor e/o
+    solver: the FP64 reliable updates still bring the solve to the target true
+    residual, within 1e-8 of the FP64 solution, in about the same iterations."""
+    conf = wl.gauge_conf(T, L, 0.35, seed=34)
+    src = wl.random_spinor(T * L ** 3 // 2, 10)
+    with Lattice(T, L) as lat:
+        lat.upload_conf(conf)
+        ref, st0 = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-22)
+        lat.set_tuning("half_arith", 1)
+        assert lat.get_tuning("half_arith") == 1
+        sol, st = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-20, precision="half")
+        assert st["true_rel_res2"] < 1e-20, st
+        assert rel(sol, ref) < 1e-8
+        assert st["iterations"] <= 1.2 * st0["iterations"] + 5, (st["iterations"], st0["iterations"])
+        lat.set_tuning("half_arith", 0)
+        sol0, _ = lat.inv_tmDkern_eoprec_square_eos_cg(KAPPA, MU, src, 100000, 1e-20, precision="half")
+        assert rel(sol0, ref) < 1e-8
+        with pytest.raises(TmError):
+            lat.set_tuning("half_arith", 2)
+
+
 def test_full_lattice_packed(cuda_device):
     """The full-lattice operator (both parities in one launch) under the packed kernel."""
     T, L = 8, 4
