@@ -104,7 +104,10 @@ def test_mixed_solve_true_residual(lat, precision):
     assert res2 < 10 * RES, res2
     assert st["true_rel_res2"] < RES
     assert float(torch.linalg.norm(sol - ref) / torch.linalg.norm(ref)) < 1e-9
-    assert abs(st["iterations"] - st64["iterations"]) <= 0.1 * st64["iterations"] + 2
+    # FP16 arithmetic perturbs the inner operator (~6e-4): more iterations between the
+    # FP64 reliable updates (113 against 98 at this volume)
+    slack = 0.3 if arith else 0.1
+    assert abs(st["iterations"] - st64["iterations"]) <= slack * st64["iterations"] + 2
     lat.set_tuning("half_arith", 0)
 
 
