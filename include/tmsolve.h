@@ -343,7 +343,8 @@ int64_t tms_hop_stage_timeouts(tms_ctx *ctx);
  * "half_arith" (FP16-spinor e/o twisted-mass solver with SU(3) links: 0 (default) FP32 arithmetic; 1 the
  * pipelined hop in FP16 arithmetic on FP16 12-real links, about 10 % faster per hop, its operator 6e-4 from
  * the FP32-arithmetic one; the solution is still brought to the target by the FP64 reliable updates, in
- * about 15 % more iterations at 32^3x64, so it is slower per solve),
+ * about 15 % more iterations at 32^3x64 with the default reliable_delta_half, 3 % more and 3-5 % less time per
+ * solve with reliable_delta_half 0.01),
  * "stream_priority" (the context's stream is recreated with this CUDA stream priority, an integer in the
  * device's range, lower first; contexts of small volumes sharing a GPU with large ones use it).  Results do not depend on the launch shapes. */
 tms_status tms_set_tuning(tms_ctx *ctx, const char *key, double value);
