@@ -23,6 +23,10 @@
 //   to a mixed-precision inner solver (same true residual, recomputed in
 //   FP64, faster): NISSA_B200_PRECISION=single|half in the environment, or
 //   nissa::b200::set_precision().
+// * Tuning knobs of the library (tms_set_tuning: launch shapes, the
+//   FP16-arithmetic hop, reliable-update factors, ...) from the environment:
+//   NISSA_B200_TUNING="key=value,key=value", applied when the context is
+//   created; an unknown key or a refused value stops the program (CRASH).
 // * Failures keep the reference's semantics: CRASH (base/debug.hpp:25) on a
 //   non-converged solve, a NaN or an invalid source, with the library's
 //   message.
@@ -32,6 +36,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <optional>
+#include <string>
 #include <vector>
 
 #include "base/debug.hpp"
@@ -66,6 +71,26 @@ namespace nissa
         if (ctx) return ctx;
         if (nranks > 1) CRASH("the B200 shim runs on one rank (nranks=%d)", nranks);
         check(tms_create4(&ctx, glbSize[0], glbSize[1], glbSize[2], glbSize[3], +1.0, 0), "tms_create4");
+        if (const char* e = std::getenv("NISSA_B200_TUNING"))
+          {
+            // "key=value,key=value"
+            std::string all(e);
+            size_t pos = 0;
+            while (pos < all.size())
+              {
+                size_t end = all.find(',', pos);
+                if (end == std::string::npos) end = all.size();
+                const std::string kv = all.substr(pos, end - pos);
+                const size_t eq = kv.find('=');
+                if (eq == std::string::npos || eq == 0) CRASH("NISSA_B200_TUNING: '%s' is not key=value", kv.c_str());
+                const std::string key = kv.substr(0, eq);
+                char* rest = nullptr;
+                const double value = std::strtod(kv.c_str() + eq + 1, &rest);
+                if (rest == kv.c_str() + eq + 1 || *rest) CRASH("NISSA_B200_TUNING: bad value in '%s'", kv.c_str());
+                check(tms_set_tuning(ctx, key.c_str(), value), "tms_set_tuning");
+                pos = end + 1;
+              }
+          }
         return ctx;
       }
 

@@ -64,6 +64,11 @@ def test_shim_full_solve_matches_reference(cuda_device):
     mix, _, out_m = oracle.run_ref("cgfull", T, L, {"conf": conf, "in": src}, shape, binary=SHIM_BIN,
                                    env={"NISSA_B200_PRECISION": "half"}, **kw)
     assert rel(mix, ref2) < 1e-8
+    # library tuning from the environment: the FP16-arithmetic hop, another launch shape
+    tuned, _, _ = oracle.run_ref("cgfull", T, L, {"conf": conf, "in": src}, shape, binary=SHIM_BIN,
+                                 env={"NISSA_B200_PRECISION": "half",
+                                      "NISSA_B200_TUNING": "half_arith=1,reliable_delta_half=0.01,tma_rows=0"}, **kw)
+    assert rel(tuned, ref2) < 1e-8
 
 
 @need
