@@ -64,7 +64,8 @@ HOP_KERNEL = {"half": "hopping kernel of the FP16 inner solver (16-bit 12-real l
 # DRAM bytes of one launch of that kernel on this workload: read from the ncu
 # summary of the current kernel under profiles/ (its "dram bytes per launch" line)
 # ncu captures of the inner hop on this workload, by (precision, launch shape)
-HOP_PROFILE = {("half", 6): "hop_kernel_fp16_pipelined_32c64.md"}
+HOP_PROFILE = {("half", 6): "hop_kernel_fp16_pipelined_32c64.md",
+               ("half-fp16-arithmetic", 6): "hop_kernel_fp16_arith_32c64.md"}
 
 
 def hop_traffic(prec, shape):
@@ -282,6 +283,11 @@ def run_ours(args):
     achieved = hop_bytes / (hop_ms * 1e-3) / 1e9
     d64_gbs = d64_bytes / (d64_ms * 1e-3) / 1e9
     traffic, traffic_src = hop_traffic(hop_prec, lat.get_tuning("hop_cfg_" + hop_prec))
+    hop_kernel_desc = HOP_KERNEL[hop_prec]
+    if args.half_arith and hop_prec == "half":
+        hop_kernel_desc = ("pipelined hopping kernel of the FP16 inner solver in FP16 arithmetic (FP16 12-real "
+                           "links) + inverse diagonal, the first half of K")
+        traffic, traffic_src = hop_traffic("half-fp16-arithmetic", 6)  # its only launch shape
 
     # --- e2e: the same columns through the C ABI from pinned host buffers -------------------
     # (tms_cg_eoprec_columns: every column's source is copied in and its solution out inside
@@ -366,9 +372,10 @@ def run_ours(args):
             base = [solve(k, precision=vp) for k in range(2)]
             variants[name]["speedup_vs_fp32_arithmetic"] = (statistics.mean(x["seconds"] for x in base) /
                                                             statistics.mean(x["seconds"] for x in vs))
+    # back to the headline's own settings
     lat.set_tuning("links_single", 1)
-    lat.set_tuning("half_arith", 0)
-    lat.set_tuning("reliable_delta_half", 0.005)
+    lat.set_tuning("half_arith", 1 if args.half_arith else 0)
+    lat.set_tuning("reliable_delta_half", 0.01 if args.half_arith else 0.005)
 
     # --- CPU baseline: one whole reference solve of column 0 (rank 0, N=1 only), and the -------
     # --- headline solution's error against it -------------------------------------------------
@@ -429,7 +436,8 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": PREC_DTYPE[prec],
+        "dtype": PREC_DTYPE[prec] if not args.half_arith else
+                 "f16 storage, f16 arithmetic hop with f32 accumulation inner / f64 reliable updates",
         "data": "synthetic (seeded gauge recipe U=exp(i eps H), point sources)",
         "config": {"workload": W["name"], "T": T, "L": L, "kappa": kappa, "mu": mu, "eps": W["eps"],
                    "residue_sq": residue, "plaquette": plaquette,
@@ -439,7 +447,7 @@ def run_ours(args):
                    "parallelism": "replicas" if ws > 1 else "1 GPU"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_per, "d2h_bytes_per_step": bytes_per,
                 "steps": e2e_steps},
-        "roofline": {"bound": "hbm", "kernel": HOP_KERNEL[hop_prec],
+        "roofline": {"bound": "hbm", "kernel": hop_kernel_desc,
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
@@ -466,7 +474,8 @@ def run_ours(args):
 
 def headline_tuning(lat, args):
     """The launch choices of the headline solve: the autotuner's (timed on this
-    lattice, cached per device and volume), or --hop-cfg / --tma-rows as given."""
+    lattice, cached per device and volume), or --hop-cfg / --tma-rows as given;
+    with --half-arith the FP16 inner hop in FP16 arithmetic (opt-in)."""
     prec = args.precision
     if args.hop_cfg >= 0:
         lat.set_tuning("hop_cfg_" + prec, args.hop_cfg)
@@ -475,6 +484,10 @@ def headline_tuning(lat, args):
         settings = {"hop_cfg_" + prec: args.hop_cfg}
         if args.tma_rows >= 0:
             settings["tma_rows"] = args.tma_rows
+        if args.half_arith:
+            lat.set_tuning("half_arith", 1)
+            lat.set_tuning("reliable_delta_half", 0.01)
+            settings.update(half_arith=1, reliable_delta_half=0.01)
         return {"source": "command line", "settings": settings}
     from nissa_b200 import tune
     t0 = time.perf_counter()
@@ -485,6 +498,11 @@ def headline_tuning(lat, args):
            "candidates": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in c.items()}
                           for c in r["candidates"]]}
     log("tuned: %s (%.1f s)" % (r["settings"], out["tuning_s"]))
+    if args.half_arith:
+        # after tuning: the FP16-arithmetic hop has one launch shape
+        lat.set_tuning("half_arith", 1)
+        lat.set_tuning("reliable_delta_half", 0.01)
+        out["settings"] = dict(out["settings"], half_arith=1, reliable_delta_half=0.01)
     return out
 
 
@@ -526,6 +544,8 @@ def run_kernel_only(args):
         lat.set_tuning("hop_cfg_" + args.kernel_only, args.hop_cfg)
     if args.tma_rows >= 0:
         lat.set_tuning("tma_rows", args.tma_rows)
+    if args.half_arith:
+        lat.set_tuning("half_arith", 1)
     if args.nrhs > 1:
         if args.mrhs:
             lat.set_tuning("mrhs_per_thread", args.mrhs)
@@ -895,6 +915,8 @@ def main():
     ap.add_argument("--mrhs", type=int, default=0, help="right-hand sides per thread of the batched kernel (tuning)")
     ap.add_argument("--hop-cfg", type=int, default=-1,
                     help="hopping-kernel launch shape of the inner precision (default: the autotuner's)")
+    ap.add_argument("--half-arith", action="store_true",
+                    help="headline with the FP16 inner hop in FP16 arithmetic (opt-in; default FP32 arithmetic)")
     ap.add_argument("--tma-rows", type=int, default=-1,
                     help="lattice rows per tile of the staged launch shape (with --hop-cfg or --kernel-only)")
     ap.add_argument("--workload", default="cg",

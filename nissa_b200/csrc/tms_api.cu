@@ -590,6 +590,9 @@ tms_status tms_bench_hop(tms_ctx* ctx, int precision, int variant, int nrep, int
                                             bytes_per_launch)
                     : bench_hop_t<PREC_F32>(ctx, links32f(ctx), variant, nrep, flush, ms_per_launch, 72.0, 96.0,
                                             bytes_per_launch);
+  if (precision == TMS_PREC_MIXED_HALF && ctx->su3 && ctx->half_arith)
+    return bench_hop_t<PREC_F16>(ctx, links16h(ctx), variant, nrep, flush, ms_per_launch, 24.0, 52.0,
+                                 bytes_per_launch);
   if (precision == TMS_PREC_MIXED_HALF)
     return ctx->su3 ? bench_hop_t<PREC_F16>(ctx, links16r(ctx), variant, nrep, flush, ms_per_launch, 24.0, 52.0,
                                             bytes_per_launch)
